@@ -1,0 +1,144 @@
+"""ccmpred_b200 -- CCMpred's pseudo-likelihood hot path on NVIDIA B200 (sm_100a).
+
+The product is ``libccmpred_b200.so`` (CUDA kernels + C ABI declared in
+``include/ccmpred_b200.h``).  This package is the Python mirror of that ABI,
+used by the tests, the benchmark and the ``torch.autograd.Function`` wrapper:
+
+* :class:`Evaluator` -- one alignment on the GPU; ``evaluate(x, g)`` is the
+  reference's evaluate callback (``src/evaluate_cpu.c:16``,
+  ``src/evaluate_cuda.c:23``) for device (torch CUDA tensors) or host (numpy)
+  buffers in the reference's padded layout;
+* :func:`calculate_weights` -- bit-exact GPU sequence reweighting
+  (``src/reweighting.c:9-58``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import CcmError, PATHS, check, lib
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+N_ALPHA = 21
+N_ALPHA_PAD = 32
+
+
+def build(verbose: bool = False) -> str:
+    """Compile libccmpred_b200.so in-tree for sm_100a (nvcc; no GPU needed)."""
+    cmd = ["make", "-C", os.path.join(HERE, "csrc"), "-j8"]
+    subprocess.run(cmd, check=True, stdout=None if verbose else subprocess.DEVNULL)
+    return _lib.LIB_PATH
+
+
+def nsingle_padded(L: int) -> int:
+    ns = L * (N_ALPHA - 1)
+    return ns + N_ALPHA_PAD - ns % N_ALPHA_PAD
+
+
+def nvar_padded(L: int) -> int:
+    return nsingle_padded(L) + L * L * N_ALPHA * N_ALPHA_PAD
+
+
+def calculate_weights(msa: np.ndarray, threshold: float = 0.8, device: int = 0) -> np.ndarray:
+    """Sequence weights on the GPU, bit-exact with the serial reference."""
+    msa = np.ascontiguousarray(msa, dtype=np.uint8)
+    N, L = msa.shape
+    w = np.empty(N, dtype=np.float32)
+    check(lib().ccm_calculate_weights(msa.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), L, N,
+                                      ctypes.c_float(threshold),
+                                      w.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), device))
+    return w
+
+
+class Evaluator:
+    """A ccm_context: the alignment, its weights and the device scratch of one path.
+
+    ``path`` is one of ``tc_bf16x2`` (default), ``tc_bf16x3``, ``simt_f32``, ``simt_f64``.
+    """
+
+    def __init__(self, msa: np.ndarray, weights: Optional[np.ndarray] = None,
+                 lambda_single: float = 0.01, lambda_pair: Optional[float] = None,
+                 path: str = "tc_bf16x2", device: int = 0, stream: Optional[int] = None):
+        self._ctx = ctypes.c_void_p(None)
+        self.msa = np.ascontiguousarray(msa, dtype=np.uint8)
+        self.N, self.L = self.msa.shape
+        self.path = path
+        self.nvar = nvar_padded(self.L)
+        self.nsp = nsingle_padded(self.L)
+        self.lambda_single = float(lambda_single)
+        self.lambda_pair = float(0.2 * (self.L - 1) if lambda_pair is None else lambda_pair)
+        opt = _lib.CcmOptions()
+        lib().ccm_options_default(ctypes.byref(opt), self.L)
+        opt.lambda_single = self.lambda_single
+        opt.lambda_pair = self.lambda_pair
+        opt.path = PATHS[path]
+        opt.device = device
+        opt.stream = stream
+        wptr = None
+        if weights is not None:
+            self.weights = np.ascontiguousarray(weights, dtype=np.float32)
+            wptr = self.weights.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        check(lib().ccm_create(ctypes.byref(self._ctx),
+                               self.msa.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
+                               self.L, self.N, wptr, ctypes.byref(opt)))
+        if weights is None:
+            self.weights = np.ones(self.N, dtype=np.float32)
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._ctx
+
+    @property
+    def stream(self) -> int:
+        return lib().ccm_stream(self._ctx)
+
+    def evaluate(self, x, g) -> float:
+        """f at x, gradient written into g.  x, g: torch CUDA tensors (float32, or
+        float64 for the simt_f64 path) or numpy float32 host arrays."""
+        fx = ctypes.c_double(0.0)
+        if isinstance(x, np.ndarray):
+            assert x.dtype == np.float32 and g.dtype == np.float32
+            assert x.flags.c_contiguous and g.flags.c_contiguous
+            check(lib().ccm_evaluate_host(self._ctx, x.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                          g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                          x.size, ctypes.byref(fx)))
+            return fx.value
+        assert x.is_cuda and g.is_cuda and x.is_contiguous() and g.is_contiguous()
+        if self.path == "simt_f64":
+            check(lib().ccm_evaluate_f64(self._ctx, x.data_ptr(), g.data_ptr(), x.numel(),
+                                         ctypes.byref(fx)))
+        else:
+            check(lib().ccm_evaluate(self._ctx, x.data_ptr(), g.data_ptr(), x.numel(),
+                                     ctypes.byref(fx)))
+        return fx.value
+
+    def evaluate_async(self, x, g) -> None:
+        check(lib().ccm_evaluate_async(self._ctx, x.data_ptr(), g.data_ptr(), x.numel()))
+
+    def result(self) -> "_lib.CcmResult":
+        r = _lib.CcmResult()
+        check(lib().ccm_get_result(self._ctx, ctypes.byref(r)))
+        return r
+
+    def close(self) -> None:
+        if self._ctx:
+            lib().ccm_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

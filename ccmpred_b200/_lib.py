@@ -1,0 +1,120 @@
+"""ctypes binding of libccmpred_b200.so (the C ABI in include/ccmpred_b200.h).
+
+The library is built in-tree by ``ccmpred_b200/csrc/Makefile`` (see
+``ccmpred_b200.build``); loading it never falls back to anything else: a
+missing library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libccmpred_b200.so")
+
+CCM_OK = 0
+CCM_ERR_INVALID = -1
+CCM_ERR_CUDA = -2
+CCM_ERR_NOMEM = -3
+CCM_ERR_DEVICE = -4
+CCM_ERR_UNSUPPORTED = -5
+
+PATH_TC_BF16X2 = 0
+PATH_TC_BF16X3 = 1
+PATH_SIMT_F32 = 2
+PATH_SIMT_F64 = 3
+PATHS = {"tc_bf16x2": PATH_TC_BF16X2, "tc_bf16x3": PATH_TC_BF16X3,
+         "simt_f32": PATH_SIMT_F32, "simt_f64": PATH_SIMT_F64}
+
+
+class CcmOptions(ctypes.Structure):
+    _fields_ = [("lambda_single", ctypes.c_float), ("lambda_pair", ctypes.c_float),
+                ("path", ctypes.c_int), ("device", ctypes.c_int), ("stream", ctypes.c_void_p)]
+
+
+class CcmResult(ctypes.Structure):
+    _fields_ = [("fx", ctypes.c_double), ("f_data", ctypes.c_double), ("reg", ctypes.c_double),
+                ("status", ctypes.c_int), ("pad", ctypes.c_int)]
+
+
+class CcmUserdata(ctypes.Structure):
+    """Layout of the reference ``userdata`` (include/ccmpred.h:39-92)."""
+    _fields_ = [("msa", ctypes.POINTER(ctypes.c_ubyte)), ("weights", ctypes.POINTER(ctypes.c_float)),
+                ("ncol", ctypes.c_int), ("nrow", ctypes.c_int), ("nsingle", ctypes.c_int),
+                ("nvar", ctypes.c_int), ("extra", ctypes.c_void_p),
+                ("lambda_single", ctypes.c_float), ("lambda_pair", ctypes.c_float),
+                ("reweighting_threshold", ctypes.c_float), ("meta_steps", ctypes.c_void_p)]
+
+
+# name -> (restype, argtypes); every symbol include/ccmpred_b200.h declares
+_vp = ctypes.c_void_p
+_f32p = ctypes.POINTER(ctypes.c_float)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_u8p = ctypes.POINTER(ctypes.c_ubyte)
+SIGNATURES = {
+    "ccm_nsingle_padded": (ctypes.c_longlong, [ctypes.c_int]),
+    "ccm_nvar_padded": (ctypes.c_longlong, [ctypes.c_int]),
+    "ccm_options_default": (None, [ctypes.POINTER(CcmOptions), ctypes.c_int]),
+    "ccm_create": (ctypes.c_int, [ctypes.POINTER(_vp), _u8p, ctypes.c_int, ctypes.c_int, _f32p,
+                                  ctypes.POINTER(CcmOptions)]),
+    "ccm_destroy": (ctypes.c_int, [_vp]),
+    "ccm_evaluate": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_longlong, _f64p]),
+    "ccm_evaluate_async": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_longlong]),
+    "ccm_evaluate_host": (ctypes.c_int, [_vp, _f32p, _f32p, ctypes.c_longlong, _f64p]),
+    "ccm_evaluate_f64": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_longlong, _f64p]),
+    "ccm_result_device": (_vp, [_vp]),
+    "ccm_get_result": (ctypes.c_int, [_vp, ctypes.POINTER(CcmResult)]),
+    "ccm_get_weights": (ctypes.c_int, [_vp, _f32p]),
+    "ccm_stream": (_vp, [_vp]),
+    "ccm_calculate_weights": (ctypes.c_int, [_u8p, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                             _f32p, ctypes.c_int]),
+    "ccm_last_error": (ctypes.c_char_p, []),
+    "ccm_debug_copy": (ctypes.c_longlong, [_vp, ctypes.c_int, _vp, ctypes.c_longlong]),
+    "ccm_set_default_path": (None, [ctypes.c_int]),
+    "ccm_init_bias": (None, [_u8p, ctypes.c_int, ctypes.c_int, _f32p]),
+    "ccm_sum_submatrices": (ctypes.c_double, [_f32p, _f32p, ctypes.c_int]),
+    "ccm_apc": (None, [_f32p, ctypes.c_int]),
+    "ccm_normalize": (ctypes.c_int, [_f32p, ctypes.c_int]),
+    "ccm_write_matrix": (ctypes.c_int, [ctypes.c_char_p, _f32p, ctypes.c_int, ctypes.c_int]),
+    "ccm_write_raw": (ctypes.c_int, [ctypes.c_char_p, _f32p, ctypes.c_int]),
+    "ccm_read_raw": (ctypes.c_int, [ctypes.c_char_p, _f32p, ctypes.c_int]),
+    "ccm_read_msa": (_u8p, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int),
+                            ctypes.POINTER(ctypes.c_int)]),
+    "ccm_free": (None, [_vp]),
+    "evaluate_cuda": (ctypes.c_float, [_vp, _vp, _vp, ctypes.c_int]),
+    "init_cuda": (ctypes.c_int, [_vp]),
+    "destroy_cuda": (ctypes.c_int, [_vp]),
+    "evaluate_b200": (ctypes.c_float, [_vp, _f32p, _f32p, ctypes.c_int]),
+    "init_b200": (ctypes.c_int, [_vp]),
+    "destroy_b200": (ctypes.c_int, [_vp]),
+}
+
+_lib = None
+
+
+class CcmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"ccmpred_b200 error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Load libccmpred_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} not found: build it with `make -C ccmpred_b200/csrc` "
+                "(or ccmpred_b200.build())")
+        l = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(l, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = l
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != CCM_OK:
+        raise CcmError(rc, lib().ccm_last_error().decode(errors="replace"))

@@ -1,0 +1,496 @@
+// C ABI of libccmpred_b200.so: context lifecycle, evaluation dispatch and the
+// reference-compatible backend triples.  See include/ccmpred_b200.h.
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "ccm_internal.cuh"
+#include "ccm_layout.cuh"
+
+namespace ccm {
+cudaError_t simt_configure_kernels();
+size_t simt_scratch_bytes(int L, int N, size_t elem);
+cudaError_t reweight_weights(const int *d_counts, float *d_w, int N, cudaStream_t stream);
+}  // namespace ccm
+
+using namespace ccm;
+
+namespace {
+
+thread_local char g_last_error[512] = "";
+int g_default_path = CCM_PATH_TC_BF16X2;
+
+int set_error(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+#define CCM_CUDA_TRY(expr)                                                                  \
+  do {                                                                                      \
+    cudaError_t _e = (expr);                                                                \
+    if (_e != cudaSuccess)                                                                  \
+      return set_error(_e == cudaErrorMemoryAllocation ? CCM_ERR_NOMEM : CCM_ERR_CUDA,      \
+                       "%s failed: %s (%s:%d)", #expr, cudaGetErrorString(_e), __FILE__,    \
+                       __LINE__);                                                           \
+  } while (0)
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn get_encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 2-D bf16 row-major [rows][cols] tensor, 128B-swizzled boxes of box_cols x box_rows.
+int make_map_bf16(CUtensorMap *map, void *base, long long rows, long long cols, int box_cols,
+                  int box_rows) {
+  EncodeTiledFn enc = get_encode_fn();
+  if (!enc) return set_error(CCM_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+  cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(CCM_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return CCM_OK;
+}
+
+// One-hot matrix O[n][s] (bf16): 1 where the state of column l(s) in row n is
+// q(s); 1 in the ones slot for every real row; 0 elsewhere (padding rows,
+// padding slots).
+__global__ void build_onehot_kernel(const uint8_t *__restrict__ msa, __nv_bfloat16 *__restrict__ O,
+                                    int L, int N, int S, int Npad) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)Npad * S) return;
+  const int n = (int)(idx / S), s = (int)(idx % S);
+  const int t = s / kGroupSlots, r = s % kGroupSlots;
+  float v = 0.0f;
+  if (n < N) {
+    if (s == kOnesSlot) {
+      v = 1.0f;
+    } else if (r < kGroupUsed) {
+      const int q = r / kGroupCols, l = t * kGroupCols + r % kGroupCols;
+      if (l < L && msa[(long long)n * L + l] == q) v = 1.0f;
+    }
+  }
+  O[idx] = __float2bfloat16_rn(v);
+}
+
+bool configured[64] = {false};
+
+int ensure_configured(int device) {
+  if (device < 0 || device >= 64) return set_error(CCM_ERR_INVALID, "bad device %d", device);
+  if (configured[device]) return CCM_OK;
+  CCM_CUDA_TRY(tc_configure_kernels());
+  CCM_CUDA_TRY(simt_configure_kernels());
+  configured[device] = true;
+  return CCM_OK;
+}
+
+int alloc_tc(ccm_context *c) {
+  c->T = n_groups(c->L);
+  c->S = c->T * kGroupSlots;
+  c->Npad = ((c->N + 127) / 128) * 128;
+  const size_t S = c->S, Np = c->Npad;
+  CCM_CUDA_TRY(cudaMalloc(&c->d_onehot, sizeof(__nv_bfloat16) * Np * S));
+  for (int i = 0; i < c->nsplit; ++i) {
+    CCM_CUDA_TRY(cudaMalloc(&c->d_wperm[i], sizeof(__nv_bfloat16) * S * S));
+    CCM_CUDA_TRY(cudaMemsetAsync(c->d_wperm[i], 0, sizeof(__nv_bfloat16) * S * S, c->stream));
+    CCM_CUDA_TRY(cudaMalloc(&c->d_r[i], sizeof(__nv_bfloat16) * Np * S));
+    CCM_CUDA_TRY(cudaMemsetAsync(c->d_r[i], 0, sizeof(__nv_bfloat16) * Np * S, c->stream));
+  }
+  const long long fwd_tiles = (long long)(c->Npad / 128) * c->T;
+  CCM_CUDA_TRY(cudaMalloc(&c->d_part_f, sizeof(double) * fwd_tiles * 4));
+  CCM_CUDA_TRY(cudaMalloc(&c->d_part_reg, sizeof(double) * kQ * c->L));
+  CCM_CUDA_TRY(cudaMalloc(&c->d_g1d, sizeof(float) * (kQ - 1) * c->L));
+
+  std::vector<int2> tiles;
+  const int p_blocks = c->S / 128;
+  for (int Q = 0; Q < c->T; ++Q)
+    for (int P = 0; P < p_blocks && P <= 2 * Q + 1; ++P) tiles.push_back(make_int2(P, Q));
+  c->n_bwd_tiles = (int)tiles.size();
+  CCM_CUDA_TRY(cudaMalloc(&c->d_bwd_tiles, sizeof(int2) * tiles.size()));
+  CCM_CUDA_TRY(cudaMemcpy(c->d_bwd_tiles, tiles.data(), sizeof(int2) * tiles.size(),
+                          cudaMemcpyHostToDevice));
+
+  const long long total = (long long)Np * S;
+  build_onehot_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c->stream>>>(
+      c->d_msa, c->d_onehot, c->L, c->N, c->S, c->Npad);
+  CCM_CUDA_TRY(cudaGetLastError());
+
+  std::memset(&c->fwd_maps, 0, sizeof(c->fwd_maps));
+  std::memset(&c->bwd_maps, 0, sizeof(c->bwd_maps));
+  int rc;
+  if ((rc = make_map_bf16(&c->fwd_maps.a, c->d_onehot, Np, S, 64, 128)) != CCM_OK) return rc;
+  if ((rc = make_map_bf16(&c->bwd_maps.o, c->d_onehot, Np, S, 64, 32)) != CCM_OK) return rc;
+  for (int i = 0; i < c->nsplit; ++i) {
+    if ((rc = make_map_bf16(&c->fwd_maps.b[i], c->d_wperm[i], S, S, 64, 64)) != CCM_OK) return rc;
+    if ((rc = make_map_bf16(&c->bwd_maps.r[i], c->d_r[i], Np, S, 64, 32)) != CCM_OK) return rc;
+  }
+  return CCM_OK;
+}
+
+int alloc_simt(ccm_context *c, size_t elem) {
+  const size_t QL = (size_t)kQ * c->L;
+  CCM_CUDA_TRY(cudaMalloc(&c->d_simt_pc, elem * (size_t)c->N * QL));
+  CCM_CUDA_TRY(cudaMalloc(&c->d_simt_g2, elem * QL * QL));
+  CCM_CUDA_TRY(cudaMalloc(&c->d_simt_g1, elem * (size_t)(kQ - 1) * c->L));
+  CCM_CUDA_TRY(cudaMalloc(&c->d_simt_part, sizeof(double) * ((size_t)c->N + QL)));
+  return CCM_OK;
+}
+
+void free_all(ccm_context *c) {
+  auto f = [](void *p) { if (p) cudaFree(p); };
+  f(c->d_msa); f(c->d_w); f(c->d_out); f(c->d_onehot);
+  for (int i = 0; i < 3; ++i) { f(c->d_wperm[i]); f(c->d_r[i]); }
+  f(c->d_part_f); f(c->d_part_reg); f(c->d_g1d); f(c->d_bwd_tiles);
+  f(c->d_simt_pc); f(c->d_simt_g2); f(c->d_simt_part); f(c->d_simt_g1);
+  f(c->d_xh); f(c->d_gh);
+  if (c->h_out) cudaFreeHost(c->h_out);
+  std::free(c->h_w);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+}
+
+int check_status(ccm_context *c) {
+  if (c->h_out->status != 0)
+    return set_error(CCM_ERR_DEVICE, "device wait timed out in %s (status 0x%x)",
+                     (c->h_out->status & kErrFwdTimeout) ? "tc_forward" : "tc_backward",
+                     c->h_out->status);
+  return CCM_OK;
+}
+
+int enqueue_eval(ccm_context *c, const float *d_x, float *d_g) {
+  CCM_CUDA_TRY(cudaMemsetAsync(c->d_out, 0, sizeof(ccm_result), c->stream));
+  cudaError_t e;
+  switch (c->path) {
+    case CCM_PATH_TC_BF16X2:
+    case CCM_PATH_TC_BF16X3: e = tc_evaluate(c, d_x, d_g); break;
+    case CCM_PATH_SIMT_F32: e = simt_evaluate(c, d_x, d_g); break;
+    case CCM_PATH_SIMT_F64:
+      return set_error(CCM_ERR_INVALID, "CCM_PATH_SIMT_F64 takes double buffers: use ccm_evaluate_f64");
+    default: return set_error(CCM_ERR_INVALID, "unknown path %d", c->path);
+  }
+  if (e != cudaSuccess)
+    return set_error(CCM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+  return CCM_OK;
+}
+
+ccm_userdata *as_ud(void *instance) { return static_cast<ccm_userdata *>(instance); }
+
+[[noreturn]] void die_ref(const char *what) {
+  // reference error behaviour: print and exit (include/evaluate_cuda_kernels.h:9)
+  printf("CUDA error in %s: %s\n", what, ccm_last_error());
+  exit(EXIT_FAILURE);
+}
+
+int init_backend(ccm_userdata *ud) {
+  if (!ud || !ud->msa || ud->ncol <= 0 || ud->nrow <= 0)
+    return set_error(CCM_ERR_INVALID, "init: invalid userdata");
+  const int L = ud->ncol, N = ud->nrow;
+  std::vector<float> w(N, 1.0f);
+  if (ud->reweighting_threshold < 1.0f) {
+    int rc = ccm_calculate_weights(ud->msa, L, N, ud->reweighting_threshold, w.data(), 0);
+    if (rc != CCM_OK) return rc;
+    float wsum = 0.0f, wmin = w[0], wmax = w[0];
+    for (int i = 0; i < N; ++i) {
+      wsum += w[i];
+      if (w[i] > wmax) wmax = w[i];
+      if (w[i] < wmin) wmin = w[i];
+    }
+    printf("Reweighted %d sequences with threshold %.1f to Beff=%g weight mean=%g, min=%g, max=%g\n",
+           N, ud->reweighting_threshold, wsum, wsum / N, wmin, wmax);
+  } else {
+    printf("Using uniform weights\n");
+  }
+  if (ud->weights) std::memcpy(ud->weights, w.data(), sizeof(float) * N);
+  ccm_options opt;
+  ccm_options_default(&opt, L);
+  opt.lambda_single = ud->lambda_single;
+  opt.lambda_pair = ud->lambda_pair;
+  opt.path = g_default_path;
+  ccm_context *ctx = nullptr;
+  int rc = ccm_create(&ctx, ud->msa, L, N, w.data(), &opt);
+  if (rc != CCM_OK) return rc;
+  ud->extra = ctx;
+  return CCM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *ccm_last_error(void) { return g_last_error; }
+
+void ccm_set_default_path(int path) { g_default_path = path; }
+
+long long ccm_nsingle_padded(int ncol) { return nsingle_padded_of(ncol); }
+long long ccm_nvar_padded(int ncol) { return nvar_padded_of(ncol); }
+
+void ccm_options_default(ccm_options *opt, int ncol) {
+  if (!opt) return;
+  opt->lambda_single = 0.01f;
+  opt->lambda_pair = 0.2f * (float)(ncol - 1);
+  opt->path = CCM_PATH_TC_BF16X2;
+  opt->device = 0;
+  opt->stream = nullptr;
+}
+
+int ccm_create(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
+               const float *weights, const ccm_options *opt) {
+  if (!out || !msa || ncol <= 0 || nrow <= 0)
+    return set_error(CCM_ERR_INVALID, "ccm_create: invalid arguments");
+  *out = nullptr;
+  ccm_options o;
+  if (opt) o = *opt; else ccm_options_default(&o, ncol);
+  if (o.path < CCM_PATH_TC_BF16X2 || o.path > CCM_PATH_SIMT_F64)
+    return set_error(CCM_ERR_INVALID, "ccm_create: unknown path %d", o.path);
+  for (long long i = 0; i < (long long)ncol * nrow; ++i)
+    if (msa[i] > 20) return set_error(CCM_ERR_INVALID, "ccm_create: MSA state %d > 20 at %lld", msa[i], i);
+  // the coupling block has 21*32*L^2 entries; keep every index in 32-bit range of int callers
+  if (nvar_padded_of(ncol) > 0x7fffffffLL)
+    return set_error(CCM_ERR_INVALID, "ccm_create: L=%d exceeds the int nvar of the reference ABI", ncol);
+
+  CCM_CUDA_TRY(cudaSetDevice(o.device));
+  cudaDeviceProp prop;
+  CCM_CUDA_TRY(cudaGetDeviceProperties(&prop, o.device));
+  if ((o.path == CCM_PATH_TC_BF16X2 || o.path == CCM_PATH_TC_BF16X3) && prop.major != 10)
+    return set_error(CCM_ERR_UNSUPPORTED, "tensor-core path needs an sm_100 device (found sm_%d%d)",
+                     prop.major, prop.minor);
+  int rc = ensure_configured(o.device);
+  if (rc != CCM_OK) return rc;
+
+  ccm_context *c = new ccm_context();
+  c->device = o.device;
+  c->num_sms = prop.multiProcessorCount;
+  c->path = o.path;
+  c->nsplit = (o.path == CCM_PATH_TC_BF16X3) ? 3 : 2;
+  c->L = ncol;
+  c->N = nrow;
+  c->nsingle = nsingle_of(ncol);
+  c->nsp = nsingle_padded_of(ncol);
+  c->nvarp = nvar_padded_of(ncol);
+  c->lambda_single = o.lambda_single;
+  c->lambda_pair = o.lambda_pair;
+  if (o.stream) {
+    c->stream = static_cast<cudaStream_t>(o.stream);
+  } else {
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete c; return set_error(CCM_ERR_CUDA, "stream: %s", cudaGetErrorString(e)); }
+    c->own_stream = true;
+  }
+  auto fail = [&](int code) { free_all(c); delete c; return code; };
+#define CCM_CTX_TRY(expr)                                                                    \
+  do {                                                                                       \
+    cudaError_t _e = (expr);                                                                 \
+    if (_e != cudaSuccess)                                                                   \
+      return fail(set_error(_e == cudaErrorMemoryAllocation ? CCM_ERR_NOMEM : CCM_ERR_CUDA,  \
+                            "%s failed: %s", #expr, cudaGetErrorString(_e)));                \
+  } while (0)
+  c->h_w = static_cast<float *>(std::malloc(sizeof(float) * nrow));
+  if (!c->h_w) return fail(set_error(CCM_ERR_NOMEM, "host weights"));
+  for (int i = 0; i < nrow; ++i) c->h_w[i] = weights ? weights[i] : 1.0f;
+  CCM_CTX_TRY(cudaMalloc(&c->d_msa, (size_t)ncol * nrow));
+  CCM_CTX_TRY(cudaMemcpyAsync(c->d_msa, msa, (size_t)ncol * nrow, cudaMemcpyHostToDevice, c->stream));
+  CCM_CTX_TRY(cudaMalloc(&c->d_w, sizeof(float) * nrow));
+  CCM_CTX_TRY(cudaMemcpyAsync(c->d_w, c->h_w, sizeof(float) * nrow, cudaMemcpyHostToDevice, c->stream));
+  CCM_CTX_TRY(cudaMalloc(&c->d_out, sizeof(ccm_result)));
+  CCM_CTX_TRY(cudaMemsetAsync(c->d_out, 0, sizeof(ccm_result), c->stream));
+  CCM_CTX_TRY(cudaMallocHost(&c->h_out, sizeof(ccm_result)));
+  c->d_status = &c->d_out->status;
+
+  if (c->path == CCM_PATH_TC_BF16X2 || c->path == CCM_PATH_TC_BF16X3) {
+    if ((rc = alloc_tc(c)) != CCM_OK) return fail(rc);
+  } else {
+    if ((rc = alloc_simt(c, c->path == CCM_PATH_SIMT_F64 ? sizeof(double) : sizeof(float))) != CCM_OK)
+      return fail(rc);
+  }
+  CCM_CTX_TRY(cudaStreamSynchronize(c->stream));
+#undef CCM_CTX_TRY
+  *out = c;
+  return CCM_OK;
+}
+
+int ccm_destroy(ccm_context *ctx) {
+  if (!ctx) return CCM_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  free_all(ctx);
+  delete ctx;
+  return CCM_OK;
+}
+
+int ccm_evaluate_async(ccm_context *c, const float *d_x, float *d_g, long long nvar) {
+  if (!c || !d_x || !d_g) return set_error(CCM_ERR_INVALID, "ccm_evaluate: null argument");
+  if (nvar != c->nvarp)
+    return set_error(CCM_ERR_INVALID, "ccm_evaluate: nvar %lld != nvar_padded %lld", nvar, c->nvarp);
+  return enqueue_eval(c, d_x, d_g);
+}
+
+int ccm_evaluate(ccm_context *c, const float *d_x, float *d_g, long long nvar, double *fx) {
+  int rc = ccm_evaluate_async(c, d_x, d_g, nvar);
+  if (rc != CCM_OK) return rc;
+  CCM_CUDA_TRY(cudaMemcpyAsync(c->h_out, c->d_out, sizeof(ccm_result), cudaMemcpyDeviceToHost, c->stream));
+  CCM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if ((rc = check_status(c)) != CCM_OK) return rc;
+  if (fx) *fx = c->h_out->fx;
+  return CCM_OK;
+}
+
+int ccm_evaluate_host(ccm_context *c, const float *x, float *g, long long nvar, double *fx) {
+  if (!c || !x || !g) return set_error(CCM_ERR_INVALID, "ccm_evaluate_host: null argument");
+  if (nvar != c->nvarp)
+    return set_error(CCM_ERR_INVALID, "ccm_evaluate_host: nvar %lld != nvar_padded %lld", nvar, c->nvarp);
+  const size_t bytes = sizeof(float) * (size_t)nvar;
+  if (!c->d_xh) {
+    CCM_CUDA_TRY(cudaMalloc(&c->d_xh, bytes));
+    CCM_CUDA_TRY(cudaMalloc(&c->d_gh, bytes));
+  }
+  CCM_CUDA_TRY(cudaMemcpyAsync(c->d_xh, x, bytes, cudaMemcpyHostToDevice, c->stream));
+  int rc = enqueue_eval(c, c->d_xh, c->d_gh);
+  if (rc != CCM_OK) return rc;
+  CCM_CUDA_TRY(cudaMemcpyAsync(g, c->d_gh, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CCM_CUDA_TRY(cudaMemcpyAsync(c->h_out, c->d_out, sizeof(ccm_result), cudaMemcpyDeviceToHost, c->stream));
+  CCM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if ((rc = check_status(c)) != CCM_OK) return rc;
+  if (fx) *fx = c->h_out->fx;
+  return CCM_OK;
+}
+
+int ccm_evaluate_f64(ccm_context *c, const double *d_x, double *d_g, long long nvar, double *fx) {
+  if (!c || !d_x || !d_g) return set_error(CCM_ERR_INVALID, "ccm_evaluate_f64: null argument");
+  if (c->path != CCM_PATH_SIMT_F64)
+    return set_error(CCM_ERR_INVALID, "ccm_evaluate_f64 needs a CCM_PATH_SIMT_F64 context");
+  if (nvar != c->nvarp)
+    return set_error(CCM_ERR_INVALID, "ccm_evaluate_f64: nvar %lld != nvar_padded %lld", nvar, c->nvarp);
+  CCM_CUDA_TRY(cudaMemsetAsync(c->d_out, 0, sizeof(ccm_result), c->stream));
+  CCM_CUDA_TRY(simt_evaluate_f64(c, d_x, d_g));
+  CCM_CUDA_TRY(cudaMemcpyAsync(c->h_out, c->d_out, sizeof(ccm_result), cudaMemcpyDeviceToHost, c->stream));
+  CCM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (fx) *fx = c->h_out->fx;
+  return CCM_OK;
+}
+
+long long ccm_debug_copy(ccm_context *c, int which, void *dst, long long bytes) {
+  if (!c) return set_error(CCM_ERR_INVALID, "ccm_debug_copy: null context");
+  const void *src = nullptr;
+  long long size = 0;
+  const long long slots = (long long)c->S;
+  if (which == 0) { src = c->d_onehot; size = 2LL * c->Npad * slots; }
+  else if (which >= 1 && which <= 3) { src = c->d_wperm[which - 1]; size = 2LL * slots * slots; }
+  else if (which >= 4 && which <= 6) { src = c->d_r[which - 4]; size = 2LL * c->Npad * slots; }
+  else if (which == 7) { src = c->d_g1d; size = 4LL * (kQ - 1) * c->L; }
+  if (!src) return set_error(CCM_ERR_INVALID, "ccm_debug_copy: buffer %d not allocated", which);
+  if (!dst) return size;
+  if (bytes < size) return set_error(CCM_ERR_INVALID, "ccm_debug_copy: need %lld bytes", size);
+  CCM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  CCM_CUDA_TRY(cudaMemcpy(dst, src, (size_t)size, cudaMemcpyDeviceToHost));
+  return CCM_OK;
+}
+
+const ccm_result *ccm_result_device(const ccm_context *c) { return c ? c->d_out : nullptr; }
+
+int ccm_get_result(ccm_context *c, ccm_result *out) {
+  if (!c || !out) return set_error(CCM_ERR_INVALID, "ccm_get_result: null argument");
+  CCM_CUDA_TRY(cudaMemcpyAsync(c->h_out, c->d_out, sizeof(ccm_result), cudaMemcpyDeviceToHost, c->stream));
+  CCM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  *out = *c->h_out;
+  return CCM_OK;
+}
+
+int ccm_get_weights(const ccm_context *c, float *w) {
+  if (!c || !w) return set_error(CCM_ERR_INVALID, "ccm_get_weights: null argument");
+  std::memcpy(w, c->h_w, sizeof(float) * c->N);
+  return CCM_OK;
+}
+
+void *ccm_stream(const ccm_context *c) { return c ? static_cast<void *>(c->stream) : nullptr; }
+
+int ccm_calculate_weights(const unsigned char *msa, int ncol, int nrow, float threshold, float *w,
+                          int device) {
+  if (!msa || !w || ncol <= 0 || nrow <= 0)
+    return set_error(CCM_ERR_INVALID, "ccm_calculate_weights: invalid arguments");
+  CCM_CUDA_TRY(cudaSetDevice(device));
+  // src/reweighting.c:10 -- threshold * ncol in float (ncol converted from uint64_t)
+  const float prod = threshold * (float)(uint64_t)ncol;
+  const int idthres = (int)ceil((double)prod);
+  cudaStream_t s;
+  CCM_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  uint8_t *d_msa = nullptr;
+  int *d_cnt = nullptr;
+  float *d_w = nullptr;
+  cudaError_t e = cudaMallocAsync(&d_msa, (size_t)ncol * nrow, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_cnt, sizeof(int) * nrow, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_w, sizeof(float) * nrow, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_msa, msa, (size_t)ncol * nrow, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = reweight_counts(d_msa, ncol, nrow, idthres, d_cnt, s);
+  if (e == cudaSuccess) e = reweight_weights(d_cnt, d_w, nrow, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w, d_w, sizeof(float) * nrow, cudaMemcpyDeviceToHost, s);
+  if (d_msa) cudaFreeAsync(d_msa, s);
+  if (d_cnt) cudaFreeAsync(d_cnt, s);
+  if (d_w) cudaFreeAsync(d_w, s);
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  if (e == cudaSuccess) e = e2;
+  if (e != cudaSuccess)
+    return set_error(CCM_ERR_CUDA, "ccm_calculate_weights: %s", cudaGetErrorString(e));
+  return CCM_OK;
+}
+
+// ------------------------------------------------------------ reference triple
+int init_cuda(void *instance) {
+  if (init_backend(as_ud(instance)) != CCM_OK) die_ref("init_cuda");
+  return EXIT_SUCCESS;
+}
+
+float evaluate_cuda(void *instance, const float *x, float *g, const int nvar) {
+  ccm_userdata *ud = as_ud(instance);
+  double fx = 0.0;
+  if (ccm_evaluate(static_cast<ccm_context *>(ud->extra), x, g, nvar, &fx) != CCM_OK)
+    die_ref("evaluate_cuda");
+  return (float)fx;
+}
+
+int destroy_cuda(void *instance) {
+  ccm_userdata *ud = as_ud(instance);
+  ccm_destroy(static_cast<ccm_context *>(ud->extra));
+  ud->extra = nullptr;
+  return EXIT_SUCCESS;
+}
+
+int init_b200(void *instance) {
+  if (init_backend(as_ud(instance)) != CCM_OK) die_ref("init_b200");
+  return 1;
+}
+
+float evaluate_b200(void *instance, const float *x, float *g, const int nvar) {
+  ccm_userdata *ud = as_ud(instance);
+  double fx = 0.0;
+  if (ccm_evaluate_host(static_cast<ccm_context *>(ud->extra), x, g, nvar, &fx) != CCM_OK)
+    die_ref("evaluate_b200");
+  return (float)fx;
+}
+
+int destroy_b200(void *instance) { return destroy_cuda(instance) == EXIT_SUCCESS ? EXIT_SUCCESS : 1; }
+
+}  // extern "C"

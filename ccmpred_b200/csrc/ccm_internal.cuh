@@ -1,0 +1,121 @@
+// Internal state of a ccm_context and the argument blocks of its kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "../../include/ccmpred_b200.h"
+
+namespace ccm {
+
+// device status bits (ccm_result.status)
+constexpr int kErrFwdTimeout = 1;
+constexpr int kErrBwdTimeout = 2;
+
+struct FwdMaps {
+  CUtensorMap a;      // one-hot O [Npad][S], box 64 (slots, K) x 128 (rows)
+  CUtensorMap b[3];   // Wperm_i  [S][S],   box 64 (out slots, N) x 64 (in slots, K)
+};
+
+struct BwdMaps {
+  CUtensorMap o;      // one-hot O [Npad][S], box 64 (slots, M/N) x 32 (rows, K)
+  CUtensorMap r[3];   // R_i       [Npad][S], same box
+};
+
+struct PrepArgs {
+  __nv_bfloat16 *wperm[3];
+  double *part_reg;
+  int L, S;
+  float lambda_pair;
+};
+
+struct FwdArgs {
+  const uint8_t *msa;
+  const float *w;
+  const float *x1;
+  __nv_bfloat16 *r[3];
+  double *part_f;
+  int *status;
+  int L, N, S, T, Npad, m_tiles;
+};
+
+struct BwdArgs {
+  const float *x2;
+  float *g2;
+  float *g1d;
+  const int2 *tiles;
+  int *status;
+  int n_tiles, L, S, Npad;
+  float lambda_pair;
+};
+
+struct FinalizeArgs {
+  const double *part_f;
+  long long n_part_f;
+  const double *part_reg;
+  long long n_part_reg;
+  const float *x1;
+  const float *g1d;
+  float *g1;
+  long long nsp;
+  int L;
+  float lambda_single, lambda_pair;
+  ccm_result *out;
+};
+
+cudaError_t tc_configure_kernels();
+cudaError_t tc_evaluate(ccm_context *c, const float *d_x, float *d_g);
+int tc_fwd_smem_bytes(int nsplit);
+int tc_bwd_smem_bytes(int nsplit);
+
+cudaError_t simt_evaluate(ccm_context *c, const float *d_x, float *d_g);
+cudaError_t simt_evaluate_f64(ccm_context *c, const double *d_x, double *d_g);
+
+cudaError_t reweight_counts(const uint8_t *d_msa, int L, int N, int idthres, int *d_counts,
+                            cudaStream_t stream);
+
+}  // namespace ccm
+
+struct ccm_context {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int path = CCM_PATH_TC_BF16X2;
+  int nsplit = 2;
+
+  int L = 0, N = 0;
+  long long nsingle = 0, nsp = 0, nvarp = 0;
+  float lambda_single = 0.01f, lambda_pair = 0.0f;
+
+  uint8_t *d_msa = nullptr;       // N x L
+  float *d_w = nullptr;           // N
+  float *h_w = nullptr;           // N (host copy)
+  ccm_result *d_out = nullptr;    // result of the last evaluation
+  ccm_result *h_out = nullptr;    // pinned host mirror
+  int *d_status = nullptr;        // == &d_out->status
+
+  // tensor-core path
+  int T = 0, S = 0, Npad = 0;
+  __nv_bfloat16 *d_onehot = nullptr;     // Npad x S
+  __nv_bfloat16 *d_wperm[3] = {nullptr, nullptr, nullptr};  // S x S
+  __nv_bfloat16 *d_r[3] = {nullptr, nullptr, nullptr};      // Npad x S
+  double *d_part_f = nullptr;
+  double *d_part_reg = nullptr;
+  float *d_g1d = nullptr;                // 20 L single-field data gradient
+  int2 *d_bwd_tiles = nullptr;
+  int n_bwd_tiles = 0;
+  ccm::FwdMaps fwd_maps;
+  ccm::BwdMaps bwd_maps;
+
+  // SIMT paths
+  void *d_simt_pc = nullptr;      // N x 21 x L probabilities (float or double)
+  void *d_simt_g2 = nullptr;      // (21L) x (21L) unsymmetrised coupling gradient
+  void *d_simt_part = nullptr;    // partial sums
+  void *d_simt_g1 = nullptr;
+
+  // host-pointer evaluation scratch
+  float *d_xh = nullptr, *d_gh = nullptr;
+};

@@ -1,0 +1,129 @@
+// Identity-threshold sequence reweighting, bit-exact with the serial reference
+// (src/reweighting.c:9-58).
+//
+// ids(i,j) = #{k : X_ik == X_jk} is counted four columns at a time on packed
+// rows (__vcmpeq4 + __popc, padding bytes subtracted), 64 x 64 row pairs per
+// block over the upper triangle of row blocks.  count_i gets +1 for every
+// j != i with ids > idthres and +2 for j == i (the reference's i <= j loop
+// visits the diagonal once and increments w[i] twice).  Counts are integers,
+// so the order of the atomic additions does not matter.
+#include <cuda_runtime.h>
+
+#include "ccm_internal.cuh"
+
+namespace ccm {
+
+constexpr int kRwTile = 64;
+constexpr int kRwChunk = 32;  // packed words per shared-memory chunk
+
+__global__ void rw_pack_kernel(const uint8_t *__restrict__ msa, uint32_t *__restrict__ packed,
+                               int L, int N, int words) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)N * words) return;
+  const int n = (int)(idx / words), wd = (int)(idx % words);
+  uint32_t v = 0;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int k = wd * 4 + e;
+    const uint32_t byte = k < L ? msa[(long long)n * L + k] : 0u;
+    v |= byte << (8 * e);
+  }
+  packed[idx] = v;
+}
+
+__global__ void __launch_bounds__(256) rw_count_kernel(const uint32_t *__restrict__ packed,
+                                                       int N, int words, int npad, int idthres,
+                                                       int *__restrict__ counts) {
+  const int IB = blockIdx.y, JB = blockIdx.x;
+  if (JB < IB) return;
+  __shared__ uint32_t As[kRwTile][kRwChunk + 1];
+  __shared__ uint32_t Bs[kRwTile][kRwChunk + 1];
+  __shared__ int ci[kRwTile], cj[kRwTile];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const int i0 = IB * kRwTile, j0 = JB * kRwTile;
+  if (threadIdx.x < kRwTile) { ci[threadIdx.x] = 0; cj[threadIdx.x] = 0; }
+  int ids[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) ids[u][v] = 0;
+
+  for (int w0 = 0; w0 < words; w0 += kRwChunk) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < kRwTile * kRwChunk; e += blockDim.x) {
+      const int r = e / kRwChunk, wd = e % kRwChunk;
+      const int ia = i0 + r, jb = j0 + r, ww = w0 + wd;
+      As[r][wd] = (ia < N && ww < words) ? packed[(long long)ia * words + ww] : 0u;
+      Bs[r][wd] = (jb < N && ww < words) ? packed[(long long)jb * words + ww] : 0u;
+    }
+    __syncthreads();
+    const int wmax = (words - w0) < kRwChunk ? (words - w0) : kRwChunk;
+    for (int wd = 0; wd < wmax; ++wd) {
+      uint32_t a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) a[u] = As[ty * 4 + u][wd];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) b[v] = Bs[tx * 4 + v][wd];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) ids[u][v] += __popc(__vcmpeq4(a[u], b[v]));
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int il = ty * 4 + u, jl = tx * 4 + v;
+      const int i = i0 + il, j = j0 + jl;
+      if (i >= N || j >= N) continue;
+      const int same = ids[u][v] / 8 - npad;
+      if (same <= idthres) continue;
+      if (IB == JB) {
+        if (i < j) { atomicAdd(&ci[il], 1); atomicAdd(&ci[jl], 1); }
+        else if (i == j) atomicAdd(&ci[il], 2);
+      } else {
+        atomicAdd(&ci[il], 1);
+        atomicAdd(&cj[jl], 1);
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kRwTile) {
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.x;
+    if (i < N && ci[threadIdx.x]) atomicAdd(&counts[i], ci[threadIdx.x]);
+    if (IB != JB && j < N && cj[threadIdx.x]) atomicAdd(&counts[j], cj[threadIdx.x]);
+  }
+}
+
+// w_i = (float)(1. / ((float)count_i - 1)) as in src/reweighting.c:43-45
+__global__ void rw_weights_kernel(const int *__restrict__ counts, float *__restrict__ w, int N) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const float cf = (float)counts[i];
+  w[i] = (float)(1.0 / (double)(cf - 1.0f));
+}
+
+cudaError_t reweight_counts(const uint8_t *d_msa, int L, int N, int idthres, int *d_counts,
+                            cudaStream_t stream) {
+  const int words = (L + 3) / 4;
+  const int npad = words * 4 - L;
+  uint32_t *packed = nullptr;
+  cudaError_t e = cudaMallocAsync(&packed, sizeof(uint32_t) * (size_t)N * words, stream);
+  if (e != cudaSuccess) return e;
+  const long long total = (long long)N * words;
+  rw_pack_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(d_msa, packed, L, N, words);
+  cudaMemsetAsync(d_counts, 0, sizeof(int) * N, stream);
+  const int nb = (N + kRwTile - 1) / kRwTile;
+  rw_count_kernel<<<dim3(nb, nb), 256, 0, stream>>>(packed, N, words, npad, idthres, d_counts);
+  cudaFreeAsync(packed, stream);
+  return cudaGetLastError();
+}
+
+cudaError_t reweight_weights(const int *d_counts, float *d_w, int N, cudaStream_t stream) {
+  rw_weights_kernel<<<(N + 255) / 256, 256, 0, stream>>>(d_counts, d_w, N);
+  return cudaGetLastError();
+}
+
+}  // namespace ccm

@@ -1,0 +1,687 @@
+// Tensor-core (tcgen05) evaluation of the pseudo-likelihood f and its gradient.
+//
+// One evaluation = four launches on the context's stream:
+//   1. tc_prep     x2 -> Wperm_i (bf16 split terms, permuted slot layout),
+//                  2*lambda2*x on the a >= 21 padding of g2, sum of x2^2 partials.
+//   2. tc_forward  logits = onehot(X) . Wperm (+ V in the epilogue), softmax over
+//                  the 21 states of every (row, column), per-row loss, and
+//                  R = w (P - onehot) split into bf16 terms.       [tcgen05 GEMM]
+//   3. tc_backward C = [O;R]^T [R;O] on the upper triangle of slot tiles, written
+//                  to g2 both as (s1,s2) and (s2,s1) with the self-edge mask and
+//                  + 2*lambda2*x; the ones slot row of C is the single-field
+//                  data gradient.                                  [tcgen05 GEMM]
+//   4. tc_finalize FP64 sums of the loss and regulariser partials, g1.
+//
+// Semantics follow src/evaluate_cpu.c:16-166 (see oracle/ccm_oracle.c for the
+// line-by-line restatement used as the checker).
+#include <cuda_bf16.h>
+
+#include "ccm_internal.cuh"
+#include "ccm_layout.cuh"
+#include "ccm_ptx.cuh"
+
+namespace ccm {
+
+// ------------------------------------------------------------------ tc_prep
+// One block per row (b,k) of the reference W matrix.  Reads that row (32 L
+// floats), writes the bf16 split terms of its 21 L real entries to row s(b,k)
+// of every Wperm_i at columns s(a,j), writes g2 = 2*lambda2*x on the padding
+// states a in [21,32), and leaves one FP64 partial of sum x^2 per row.
+template <int NSPLIT>
+__global__ void __launch_bounds__(256) tc_prep_kernel(const float *__restrict__ x2,
+                                                      float *__restrict__ g2, PrepArgs args) {
+  const int L = args.L;
+  const int row = blockIdx.x;           // b*L + k
+  const int b = row / L, k = row % L;
+  const long long base = (long long)row * kQPad * L;
+  const long long srow = (long long)slot_of(b, k) * args.S;
+  const float two_l2 = 2.0f * args.lambda_pair;
+  double acc = 0.0;
+  for (int a = 0; a < kQPad; ++a) {
+    const float *xr = x2 + base + (long long)a * L;
+    if (a < kQ) {
+      for (int j = threadIdx.x; j < L; j += blockDim.x) {
+        const float v = xr[j];
+        acc += (double)v * (double)v;
+        const long long dst = srow + slot_of(a, j);
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        const float r1 = v - __bfloat162float(h);
+        const __nv_bfloat16 l1 = __float2bfloat16_rn(r1);
+        args.wperm[0][dst] = h;
+        args.wperm[1][dst] = l1;
+        if (NSPLIT > 2) {
+          const float r2 = r1 - __bfloat162float(l1);
+          args.wperm[2][dst] = __float2bfloat16_rn(r2);
+        }
+      }
+    } else {
+      float *gr = g2 + base + (long long)a * L;
+      for (int j = threadIdx.x; j < L; j += blockDim.x) {
+        const float v = xr[j];
+        acc += (double)v * (double)v;
+        gr[j] = two_l2 * v;
+      }
+    }
+  }
+  // block reduction, fixed order
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    args.part_reg[row] = s;
+  }
+}
+
+// --------------------------------------------------------------- tc_forward
+constexpr int kFwdBM = 128, kFwdBN = 256, kFwdBK = 64;
+constexpr int kFwdStages = 2;
+constexpr int kThreads = 192;  // warp 0: TMA, warp 1: MMA, warps 2-5: epilogue
+
+template <int NSPLIT>
+struct FwdSmem {
+  static constexpr int kABytes = kFwdBM * kFwdBK * 2;            // 16 KB
+  static constexpr int kBBytes = kFwdBN * kFwdBK * 2;            // 32 KB per term
+  static constexpr int kStage = kABytes + NSPLIT * kBBytes;
+  static constexpr int kBarOff = kFwdStages * kStage;
+  static constexpr int kVOff = kBarOff + 256;
+  static constexpr int kTotal = kVOff + 240 * 4 + 1024;            // + alignment slack
+};
+
+__device__ __forceinline__ uint8_t *align1024(uint8_t *p) {
+  const uint32_t s = smem_u32(p);
+  return p + ((1024u - (s & 1023u)) & 1023u);
+}
+
+__device__ __forceinline__ void record_error(int *status, int bit, int *abort_flag) {
+  atomicOr(status, bit);
+  *reinterpret_cast<volatile int *>(abort_flag) = 1;
+}
+
+__device__ __forceinline__ bool aborted(const int *abort_flag) {
+  return *reinterpret_cast<const volatile int *>(abort_flag) != 0;
+}
+
+template <int NSPLIT>
+__global__ void __launch_bounds__(kThreads, 1)
+    tc_forward_kernel(const __grid_constant__ FwdMaps maps, FwdArgs args) {
+  using SM = FwdSmem<NSPLIT>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = align1024(smem_raw);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + SM::kBarOff);
+  uint64_t *empty = full + kFwdStages;
+  uint64_t *tfull = empty + kFwdStages;
+  uint64_t *tempty = tfull + 2;
+  uint64_t *drain = tempty + 2;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+  float *Vs = reinterpret_cast<float *>(smem + SM::kVOff);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n_tiles = args.m_tiles * args.T;
+  const int k_blocks = args.S / kFwdBK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kFwdStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+    for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 4); }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&maps.a);
+    for (int i = 0; i < NSPLIT; ++i) prefetch_tmap(&maps.b[i]);
+  }
+  if (warp == 1) { tmem_alloc(tmem_slot, 512); tmem_relinquish(); }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---------------- TMA producer
+      uint32_t it = 0;
+      for (int tile = blockIdx.x; tile < n_tiles && !aborted(abort_flag); tile += gridDim.x) {
+        const int m = tile % args.m_tiles, t = tile / args.m_tiles;
+        for (int kb = 0; kb < k_blocks; ++kb, ++it) {
+          const int stage = it % kFwdStages;
+          const uint32_t round = it / kFwdStages;
+          if (!mbar_wait(&empty[stage], (round & 1) ^ 1)) {
+            record_error(args.status, kErrFwdTimeout, abort_flag);
+            break;
+          }
+          uint8_t *sa = smem + stage * SM::kStage;
+          mbar_arrive_expect_tx(&full[stage], SM::kStage);
+          tma_load_2d(sa, &maps.a, &full[stage], kb * kFwdBK, m * kFwdBM);
+          for (int i = 0; i < NSPLIT; ++i) {
+            uint8_t *sb = sa + SM::kABytes + i * SM::kBBytes;
+            for (int c = 0; c < 4; ++c)
+              tma_load_2d(sb + c * (kFwdBK * 128), &maps.b[i], &full[stage],
+                          t * kFwdBN + c * 64, kb * kFwdBK);
+          }
+        }
+      }
+      // drain: every issued load must land before the CTA may exit
+      const uint32_t issued = it;
+      for (uint32_t r = (issued > kFwdStages ? issued - kFwdStages : 0); r < issued; ++r)
+        if (!mbar_wait(&full[r % kFwdStages], (r / kFwdStages) & 1)) {
+          record_error(args.status, kErrFwdTimeout, abort_flag);
+          break;
+        }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---------------- MMA issuer
+      constexpr uint32_t idesc = idesc_bf16_f32(kFwdBM, kFwdBN, 0, 1);
+      uint32_t it = 0;
+      int local = 0;
+      for (int tile = blockIdx.x; tile < n_tiles && !aborted(abort_flag);
+           tile += gridDim.x, ++local) {
+        const int acc = local & 1;
+        const uint32_t use = local >> 1;
+        if (!mbar_wait(&tempty[acc], (use & 1) ^ 1)) {
+          record_error(args.status, kErrFwdTimeout, abort_flag);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem_base + acc * kFwdBN;
+        bool ok = true;
+        for (int kb = 0; kb < k_blocks; ++kb, ++it) {
+          const int stage = it % kFwdStages;
+          const uint32_t round = it / kFwdStages;
+          if (!mbar_wait(&full[stage], round & 1)) {
+            record_error(args.status, kErrFwdTimeout, abort_flag);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(smem + stage * SM::kStage);
+          const uint32_t b0 = a0 + SM::kABytes;
+#pragma unroll
+          for (int k16 = 0; k16 < kFwdBK / 16; ++k16) {
+            const uint64_t ad = sdesc_sw128(a0 + k16 * 32, 16, 1024);
+#pragma unroll
+            for (int i = 0; i < NSPLIT; ++i) {
+              const uint64_t bd =
+                  sdesc_sw128(b0 + i * SM::kBBytes + k16 * 16 * 128, kFwdBK * 128, 1024);
+              umma_bf16(d, ad, bd, idesc, (kb | k16 | i) != 0);
+            }
+          }
+          umma_commit(&empty[stage]);
+        }
+        if (!ok) break;
+        umma_commit(&tfull[acc]);
+      }
+      umma_commit(drain);
+      if (!mbar_wait(drain, 0)) record_error(args.status, kErrFwdTimeout, abort_flag);
+    }
+  } else {
+    // ---------------- epilogue: 4 warps, warp w owns TMEM lanes 32*(w%4) ...
+    const int q = warp & 3;
+    const int ethr = threadIdx.x - 64;
+    const int L = args.L;
+    int local = 0;
+    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++local) {
+      // all four epilogue warps agree here: every one finished the previous
+      // tile (so Vs may be overwritten) and none has seen an abort
+      if (named_bar_or(1, 128, aborted(abort_flag))) break;
+      const int acc = local & 1;
+      const uint32_t use = local >> 1;
+      const int m = tile % args.m_tiles, t = tile / args.m_tiles;
+      const int j0 = t * kGroupCols;
+      for (int idx = ethr; idx < (kQ - 1) * kGroupCols; idx += 128) {
+        const int a = idx / kGroupCols, j = j0 + idx % kGroupCols;
+        Vs[idx] = (j < L) ? args.x1[a * L + j] : 0.0f;
+      }
+      named_bar_sync(1, 128);
+
+      const int n = m * kFwdBM + q * 32 + lane;
+      const bool live = n < args.N;
+      const float wn = live ? args.w[n] : 0.0f;
+      int xr[kGroupCols];
+#pragma unroll
+      for (int jj = 0; jj < kGroupCols; ++jj) {
+        const int j = j0 + jj;
+        xr[jj] = (live && j < L) ? (int)args.msa[(long long)n * L + j] : -1;
+      }
+      bool ok = mbar_wait(&tfull[acc], use & 1);
+      if (__any_sync(0xffffffffu, !ok)) {
+        // leave through the agreement barrier at the top of the loop
+        if (lane == 0) record_error(args.status, kErrFwdTimeout, abort_flag);
+        continue;
+      }
+      tc_fence_after();
+      const uint32_t taddr = tmem_base + acc * kFwdBN + ((uint32_t)(q * 32) << 16);
+      // volatile: re-read V from shared memory in every pass instead of keeping
+      // 240 values live in registers across the three passes
+      const volatile float *Vv = Vs;
+
+      float mx[kGroupCols], tg[kGroupCols], se[kGroupCols];
+#pragma unroll
+      for (int jj = 0; jj < kGroupCols; ++jj) { mx[jj] = -INFINITY; tg[jj] = 0.0f; se[jj] = 0.0f; }
+
+      // pass A: max over states, logit of the observed state
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        uint32_t v[32];
+        __syncwarp();
+        tmem_ld32(taddr + c * 32, v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          const int col = c * 32 + i;
+          if (col < kGroupUsed) {
+            const int a = col / kGroupCols, jj = col % kGroupCols;
+            const float z = __uint_as_float(v[i]) + (a < kQ - 1 ? Vv[a * kGroupCols + jj] : 0.0f);
+            mx[jj] = fmaxf(mx[jj], z);
+            if (xr[jj] == a) tg[jj] = z;
+          }
+        }
+      }
+      // pass B: sum of exp
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        uint32_t v[32];
+        __syncwarp();
+        tmem_ld32(taddr + c * 32, v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          const int col = c * 32 + i;
+          if (col < kGroupUsed) {
+            const int a = col / kGroupCols, jj = col % kGroupCols;
+            const float z = __uint_as_float(v[i]) + (a < kQ - 1 ? Vv[a * kGroupCols + jj] : 0.0f);
+            se[jj] += expf(z - mx[jj]);
+          }
+        }
+      }
+      float lse[kGroupCols];
+      double floss = 0.0;
+#pragma unroll
+      for (int jj = 0; jj < kGroupCols; ++jj) {
+        lse[jj] = mx[jj] + logf(se[jj]);
+        if (xr[jj] >= 0) floss += (double)(wn * (lse[jj] - tg[jj]));
+      }
+      // pass C: R = w (P - onehot), split into bf16 terms, stored row-major [n][slot]
+      const long long rbase = (long long)n * args.S + (long long)t * kGroupSlots;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        uint32_t v[32];
+        __syncwarp();
+        tmem_ld32(taddr + c * 32, v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {        // 8 slots -> one 16-byte store per term
+          uint32_t ph[4], pl[4], pl2[4];
+#pragma unroll
+          for (int e2 = 0; e2 < 4; ++e2) {
+            uint32_t hh = 0, ll = 0, l2 = 0;
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int i = u * 8 + e2 * 2 + e;
+              const int col = c * 32 + i;
+              float r = 0.0f;
+              if (col < kGroupUsed) {
+                const int a = col / kGroupCols, jj = col % kGroupCols;
+                const float z =
+                    __uint_as_float(v[i]) + (a < kQ - 1 ? Vv[a * kGroupCols + jj] : 0.0f);
+                if (xr[jj] >= 0) r = wn * (expf(z - lse[jj]) - (xr[jj] == a ? 1.0f : 0.0f));
+              }
+              const __nv_bfloat16 hb = __float2bfloat16_rn(r);
+              const float rr = r - __bfloat162float(hb);
+              const __nv_bfloat16 lb = __float2bfloat16_rn(rr);
+              hh |= (uint32_t)__bfloat16_as_ushort(hb) << (16 * e);
+              ll |= (uint32_t)__bfloat16_as_ushort(lb) << (16 * e);
+              if (NSPLIT > 2)
+                l2 |= (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(rr - __bfloat162float(lb)))
+                      << (16 * e);
+            }
+            ph[e2] = hh; pl[e2] = ll; pl2[e2] = l2;
+          }
+          const long long off = rbase + c * 32 + u * 8;
+          *reinterpret_cast<uint4 *>(args.r[0] + off) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+          *reinterpret_cast<uint4 *>(args.r[1] + off) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+          if (NSPLIT > 2)
+            *reinterpret_cast<uint4 *>(args.r[2] + off) = make_uint4(pl2[0], pl2[1], pl2[2], pl2[3]);
+        }
+      }
+      // accumulator may be reused by the MMA warp
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[acc]);
+      // loss partial, one per (tile, warp), summed in fixed order by tc_finalize
+      for (int o = 16; o > 0; o >>= 1) floss += __shfl_xor_sync(0xffffffffu, floss, o);
+      if (lane == 0) args.part_f[(long long)tile * 4 + q] = floss;
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem_base, 512);
+  }
+}
+
+// -------------------------------------------------------------- tc_backward
+constexpr int kBwdBM = 128, kBwdBN = 256, kBwdBK = 32;
+
+template <int NSPLIT>
+struct BwdSmem {
+  static constexpr int kStages = NSPLIT == 2 ? 3 : 2;
+  static constexpr int kChunk = kBwdBK * 128;                    // 64 slots x BK rows = 4 KB
+  static constexpr int kA = 2 * kChunk;                          // 128 slots
+  static constexpr int kB = 4 * kChunk;                          // 256 slots
+  // stage: O_P | R_P[i] | O_Q | R_Q[i]
+  static constexpr int kOffOP = 0;
+  static constexpr int kOffRP = kA;
+  static constexpr int kOffOQ = kA + NSPLIT * kA;
+  static constexpr int kOffRQ = kOffOQ + kB;
+  static constexpr int kStage = kOffRQ + NSPLIT * kB;
+  static constexpr int kBarOff = kStages * kStage;
+  static constexpr int kTotal = kBarOff + 256 + 1024;
+};
+
+template <int NSPLIT>
+__global__ void __launch_bounds__(kThreads, 1)
+    tc_backward_kernel(const __grid_constant__ BwdMaps maps, BwdArgs args) {
+  using SM = BwdSmem<NSPLIT>;
+  constexpr int kStages = SM::kStages;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = align1024(smem_raw);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + SM::kBarOff);
+  uint64_t *empty = full + kStages;
+  uint64_t *tfull = empty + kStages;
+  uint64_t *tempty = tfull + 2;
+  uint64_t *drain = tempty + 2;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n_tiles = args.n_tiles;
+  const int k_blocks = args.Npad / kBwdBK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+    for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 4); }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&maps.o);
+    for (int i = 0; i < NSPLIT; ++i) prefetch_tmap(&maps.r[i]);
+  }
+  if (warp == 1) { tmem_alloc(tmem_slot, 512); tmem_relinquish(); }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t it = 0;
+      for (int tile = blockIdx.x; tile < n_tiles && !aborted(abort_flag); tile += gridDim.x) {
+        const int2 pq = args.tiles[tile];
+        const int xP = pq.x * kBwdBM, xQ = pq.y * kBwdBN;
+        for (int kb = 0; kb < k_blocks; ++kb, ++it) {
+          const int stage = it % kStages;
+          const uint32_t round = it / kStages;
+          if (!mbar_wait(&empty[stage], (round & 1) ^ 1)) {
+            record_error(args.status, kErrBwdTimeout, abort_flag);
+            break;
+          }
+          uint8_t *st = smem + stage * SM::kStage;
+          const int y = kb * kBwdBK;
+          mbar_arrive_expect_tx(&full[stage], SM::kStage);
+          for (int c = 0; c < 2; ++c)
+            tma_load_2d(st + SM::kOffOP + c * SM::kChunk, &maps.o, &full[stage], xP + 64 * c, y);
+          for (int i = 0; i < NSPLIT; ++i)
+            for (int c = 0; c < 2; ++c)
+              tma_load_2d(st + SM::kOffRP + i * SM::kA + c * SM::kChunk, &maps.r[i], &full[stage],
+                          xP + 64 * c, y);
+          for (int c = 0; c < 4; ++c)
+            tma_load_2d(st + SM::kOffOQ + c * SM::kChunk, &maps.o, &full[stage], xQ + 64 * c, y);
+          for (int i = 0; i < NSPLIT; ++i)
+            for (int c = 0; c < 4; ++c)
+              tma_load_2d(st + SM::kOffRQ + i * SM::kB + c * SM::kChunk, &maps.r[i], &full[stage],
+                          xQ + 64 * c, y);
+        }
+      }
+      const uint32_t issued = it;
+      for (uint32_t r = (issued > (uint32_t)kStages ? issued - kStages : 0); r < issued; ++r)
+        if (!mbar_wait(&full[r % kStages], (r / kStages) & 1)) {
+          record_error(args.status, kErrBwdTimeout, abort_flag);
+          break;
+        }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_bf16_f32(kBwdBM, kBwdBN, 1, 1);
+      uint32_t it = 0;
+      int local = 0;
+      for (int tile = blockIdx.x; tile < n_tiles && !aborted(abort_flag);
+           tile += gridDim.x, ++local) {
+        const int acc = local & 1;
+        const uint32_t use = local >> 1;
+        if (!mbar_wait(&tempty[acc], (use & 1) ^ 1)) {
+          record_error(args.status, kErrBwdTimeout, abort_flag);
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem_base + acc * kBwdBN;
+        bool ok = true;
+        for (int kb = 0; kb < k_blocks; ++kb, ++it) {
+          const int stage = it % kStages;
+          const uint32_t round = it / kStages;
+          if (!mbar_wait(&full[stage], round & 1)) {
+            record_error(args.status, kErrBwdTimeout, abort_flag);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t s0 = smem_u32(smem + stage * SM::kStage);
+#pragma unroll
+          for (int k16 = 0; k16 < kBwdBK / 16; ++k16) {
+            const uint32_t ko = k16 * 16 * 128;
+            const uint64_t dOP = sdesc_sw128(s0 + SM::kOffOP + ko, SM::kChunk, 1024);
+            const uint64_t dOQ = sdesc_sw128(s0 + SM::kOffOQ + ko, SM::kChunk, 1024);
+#pragma unroll
+            for (int i = 0; i < NSPLIT; ++i) {
+              const uint64_t dRQ = sdesc_sw128(s0 + SM::kOffRQ + i * SM::kB + ko, SM::kChunk, 1024);
+              umma_bf16(d, dOP, dRQ, idesc, (kb | k16 | i) != 0);
+            }
+#pragma unroll
+            for (int i = 0; i < NSPLIT; ++i) {
+              const uint64_t dRP = sdesc_sw128(s0 + SM::kOffRP + i * SM::kA + ko, SM::kChunk, 1024);
+              umma_bf16(d, dRP, dOQ, idesc, 1);
+            }
+          }
+          umma_commit(&empty[stage]);
+        }
+        if (!ok) break;
+        umma_commit(&tfull[acc]);
+      }
+      umma_commit(drain);
+      if (!mbar_wait(drain, 0)) record_error(args.status, kErrBwdTimeout, abort_flag);
+    }
+  } else {
+    const int q = warp & 3;
+    const int L = args.L;
+    const float two_l2 = 2.0f * args.lambda_pair;
+    const float *__restrict__ x2 = args.x2;
+    float *__restrict__ g2 = args.g2;
+    int local = 0;
+    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++local) {
+      if (__shfl_sync(0xffffffffu, aborted(abort_flag) ? 1 : 0, 0)) break;
+      const int acc = local & 1;
+      const uint32_t use = local >> 1;
+      const int2 pq = args.tiles[tile];
+      const int s1 = pq.x * kBwdBM + q * 32 + lane;
+      const int t1 = s1 / kGroupSlots, r1 = s1 % kGroupSlots;
+      const int b = r1 / kGroupCols, k = t1 * kGroupCols + r1 % kGroupCols;
+      const bool valid1 = r1 < kGroupUsed && k < L;
+      const long long rowd = valid1 ? x2_index(b, k, 0, 0, L) : 0;  // + a*L + j
+      const long long colt = (long long)b * L + k;                  // + ((a*L+j)*32)*L
+      const int sQ = pq.y * kBwdBN;
+      const int jQ = pq.y * kGroupCols;
+
+      bool ok = mbar_wait(&tfull[acc], use & 1);
+      if (__any_sync(0xffffffffu, !ok)) {
+        if (lane == 0) record_error(args.status, kErrBwdTimeout, abort_flag);
+        break;
+      }
+      tc_fence_after();
+      const uint32_t taddr = tmem_base + acc * kBwdBN + ((uint32_t)(q * 32) << 16);
+#pragma unroll 1
+      for (int c = 0; c < 8; ++c) {
+        uint32_t v[32];
+        __syncwarp();
+        tmem_ld32(taddr + c * 32, v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          const int r2 = c * 32 + i;
+          const int s2 = sQ + r2;
+          const int a = r2 / kGroupCols, j = jQ + r2 % kGroupCols;
+          const bool valid2 = r2 < kGroupUsed && j < L;
+          const float cval = __uint_as_float(v[i]);
+          if (s1 <= s2) {
+            if (valid1 && valid2) {
+              const float gd = (k == j) ? 0.0f : cval;
+              const long long id = rowd + (long long)a * L + j;
+              g2[id] = gd + two_l2 * x2[id];
+              if (s1 != s2) {
+                const long long it2 = ((long long)a * L + j) * kQPad * L + colt;
+                g2[it2] = gd + two_l2 * x2[it2];
+              }
+            } else if (s1 == kOnesSlot && valid2 && a < kQ - 1) {
+              args.g1d[a * L + j] = cval;
+            } else if (s2 == kOnesSlot && valid1 && b < kQ - 1) {
+              args.g1d[b * L + k] = cval;
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[acc]);
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem_base, 512);
+  }
+}
+
+// -------------------------------------------------------------- tc_finalize
+// fx = sum(loss partials) + lambda1 sum V^2 + 0.5 lambda2 sum x2^2 (all in FP64,
+// fixed summation order); g1 = g1d + 2 lambda1 V, g1 padding = 0
+// (src/evaluate_cpu.c:151-163).
+__global__ void __launch_bounds__(1024) tc_finalize_kernel(FinalizeArgs args) {
+  __shared__ double red[32];
+  double acc_f = 0.0, acc_r2 = 0.0, acc_r1 = 0.0;
+  for (long long i = threadIdx.x; i < args.n_part_f; i += blockDim.x) acc_f += args.part_f[i];
+  for (long long i = threadIdx.x; i < args.n_part_reg; i += blockDim.x) acc_r2 += args.part_reg[i];
+  const long long ns = nsingle_of(args.L);
+  const float two_l1 = 2.0f * args.lambda_single;
+  for (long long v = threadIdx.x; v < args.nsp; v += blockDim.x) {
+    if (v < ns) {
+      const float xv = args.x1[v];
+      acc_r1 += (double)xv * (double)xv;
+      if (args.g1 != nullptr) args.g1[v] = args.g1d[v] + two_l1 * xv;
+    } else if (args.g1 != nullptr) {
+      args.g1[v] = 0.0f;
+    }
+  }
+  auto block_sum = [&](double x) -> double {
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    return s;
+  };
+  const double F = block_sum(acc_f);
+  const double R2 = block_sum(acc_r2);
+  const double R1 = block_sum(acc_r1);
+  if (threadIdx.x == 0) {
+    const double fx = F + (double)args.lambda_single * R1 + 0.5 * (double)args.lambda_pair * R2;
+    args.out->fx = fx;
+    args.out->f_data = F;
+    args.out->reg = fx - F;
+  }
+}
+
+// ---------------------------------------------------------------- launchers
+template <int NSPLIT>
+static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
+  const int L = c->L;
+  const float *x1 = d_x;
+  const float *x2 = d_x + c->nsp;
+  float *g2 = d_g + c->nsp;
+
+  PrepArgs pa{};
+  pa.L = L; pa.S = c->S; pa.lambda_pair = c->lambda_pair; pa.part_reg = c->d_part_reg;
+  for (int i = 0; i < 3; ++i) pa.wperm[i] = c->d_wperm[i];
+  tc_prep_kernel<NSPLIT><<<kQ * L, 256, 0, c->stream>>>(x2, g2, pa);
+
+  FwdArgs fa{};
+  fa.msa = c->d_msa; fa.w = c->d_w; fa.x1 = x1; fa.part_f = c->d_part_f; fa.status = c->d_status;
+  for (int i = 0; i < 3; ++i) fa.r[i] = c->d_r[i];
+  fa.L = L; fa.N = c->N; fa.S = c->S; fa.T = c->T; fa.Npad = c->Npad; fa.m_tiles = c->Npad / kFwdBM;
+  const int fwd_tiles = fa.m_tiles * c->T;
+  const int fwd_grid = fwd_tiles < c->num_sms ? fwd_tiles : c->num_sms;
+  tc_forward_kernel<NSPLIT><<<fwd_grid, kThreads, FwdSmem<NSPLIT>::kTotal, c->stream>>>(
+      c->fwd_maps, fa);
+
+  BwdArgs ba{};
+  ba.x2 = x2; ba.g2 = g2; ba.g1d = c->d_g1d; ba.tiles = c->d_bwd_tiles;
+  ba.n_tiles = c->n_bwd_tiles; ba.status = c->d_status; ba.L = L; ba.S = c->S; ba.Npad = c->Npad;
+  ba.lambda_pair = c->lambda_pair;
+  const int bwd_grid = c->n_bwd_tiles < c->num_sms ? c->n_bwd_tiles : c->num_sms;
+  tc_backward_kernel<NSPLIT><<<bwd_grid, kThreads, BwdSmem<NSPLIT>::kTotal, c->stream>>>(
+      c->bwd_maps, ba);
+
+  FinalizeArgs za{};
+  za.part_f = c->d_part_f; za.n_part_f = (long long)fwd_tiles * 4;
+  za.part_reg = c->d_part_reg; za.n_part_reg = (long long)kQ * L;
+  za.x1 = x1; za.g1d = c->d_g1d; za.g1 = d_g; za.L = L; za.nsp = c->nsp;
+  za.lambda_single = c->lambda_single; za.lambda_pair = c->lambda_pair; za.out = c->d_out;
+  tc_finalize_kernel<<<1, 1024, 0, c->stream>>>(za);
+  return cudaGetLastError();
+}
+
+cudaError_t tc_configure_kernels() {
+  cudaError_t e;
+  e = cudaFuncSetAttribute(tc_forward_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           FwdSmem<2>::kTotal);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(tc_forward_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           FwdSmem<3>::kTotal);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(tc_backward_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           BwdSmem<2>::kTotal);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(tc_backward_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              BwdSmem<3>::kTotal);
+}
+
+cudaError_t tc_evaluate(ccm_context *c, const float *d_x, float *d_g) {
+  return c->nsplit == 3 ? launch_tc<3>(c, d_x, d_g) : launch_tc<2>(c, d_x, d_g);
+}
+
+int tc_fwd_smem_bytes(int nsplit) { return nsplit == 3 ? FwdSmem<3>::kTotal : FwdSmem<2>::kTotal; }
+int tc_bwd_smem_bytes(int nsplit) { return nsplit == 3 ? BwdSmem<3>::kTotal : BwdSmem<2>::kTotal; }
+
+}  // namespace ccm

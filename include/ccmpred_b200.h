@@ -1,0 +1,204 @@
+/*
+ * ccmpred_b200.h -- C ABI of libccmpred_b200.so, a B200 (sm_100a) implementation
+ * of CCMpred's pseudo-likelihood objective + gradient.
+ *
+ * Two layers:
+ *
+ *  1. The reference's own backend triple, drop-in compatible with
+ *     include/evaluate_cuda.h:8-17 (evaluate_cuda/init_cuda/destroy_cuda, the
+ *     libconjugrad evaluate callback with DEVICE x and g) and, for host
+ *     pointers, the shape of include/evaluate_cpu.h:21-30 (evaluate_b200 etc.).
+ *     `instance` points at a struct with the layout of the reference's
+ *     `userdata` (include/ccmpred.h:39-92), declared here as ccm_userdata.
+ *     As in the reference (CHECK_ERR, include/evaluate_cuda_kernels.h:9), these
+ *     print the error and exit(EXIT_FAILURE) on failure.
+ *
+ *  2. A context API (ccm_*) with explicit sizes and status codes, one context
+ *     per alignment, no process globals, one CUDA stream per context.
+ *
+ * Parameter vector layout (both layers): the reference's padded layout,
+ * include/ccmpred.h:1-17 with PADDING on (N_ALPHA_PAD = 32):
+ *   x[a*L + j]                          single field V(j,a), a < 20
+ *   x[nsingle .. nsingle_padded)        padding (gradient written as 0)
+ *   x[nsingle_padded + ((b*L+k)*32 + a)*L + j]   coupling W(b,k,a,j)
+ * with nsingle = 20 L and nsingle_padded = nsingle + 32 - nsingle % 32
+ * (src/ccmpred.c:388-390); nvar_padded = nsingle_padded + 21*32*L*L.
+ * The gradient is the reference's: the coupling part is the derivative along
+ * the tied direction W(b,k,a,j) = W(a,j,b,k) with zeroed self-edge blocks
+ * (src/evaluate_cpu.c:131-163).
+ */
+#ifndef CCMPRED_B200_H
+#define CCMPRED_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define CCM_API __attribute__((visibility("default")))
+#else
+#define CCM_API
+#endif
+
+#define CCM_N_ALPHA 21
+#define CCM_N_ALPHA_PAD 32
+
+/* status codes of the ccm_* API */
+#define CCM_OK 0
+#define CCM_ERR_INVALID (-1)      /* bad argument (sizes, null pointers, nvar mismatch) */
+#define CCM_ERR_CUDA (-2)         /* a CUDA runtime call failed; see ccm_last_error() */
+#define CCM_ERR_NOMEM (-3)        /* device allocation failed */
+#define CCM_ERR_DEVICE (-4)       /* a kernel reported a bounded-wait timeout */
+#define CCM_ERR_UNSUPPORTED (-5)  /* no sm_100 device / unsupported option */
+
+/* evaluation paths */
+#define CCM_PATH_TC_BF16X2 0 /* tcgen05, W and R split into hi+lo bf16, f32 accumulate */
+#define CCM_PATH_TC_BF16X3 1 /* tcgen05, three bf16 terms (hi+mid+lo) */
+#define CCM_PATH_SIMT_F32 2  /* plain FP32 CUDA-core path (no tensor cores) */
+#define CCM_PATH_SIMT_F64 3  /* FP64 CUDA-core path (gradient checks) */
+
+typedef struct ccm_context ccm_context;
+
+typedef struct ccm_options {
+	float lambda_single; /* default 0.01 (src/ccmpred.c:222) */
+	float lambda_pair;   /* default 0.2 * (L - 1) (src/ccmpred.c:224,502-503) */
+	int path;            /* CCM_PATH_* ; default CCM_PATH_TC_BF16X2 */
+	int device;          /* CUDA device ordinal; default 0 */
+	void *stream;        /* cudaStream_t to run on, or NULL for a private stream */
+} ccm_options;
+
+/* Result of the last evaluation, as kept on the device. */
+typedef struct ccm_result {
+	double fx;     /* f = data term + regulariser */
+	double f_data; /* sum_n w_n sum_j (lse - logit of observed state) */
+	double reg;    /* lambda1 sum V^2 + 0.5 lambda2 sum W^2 over all padded slots */
+	int status;    /* device error bits, 0 when clean */
+	int pad;
+} ccm_result;
+
+/* Reference `userdata` (include/ccmpred.h:39-92), float build. */
+typedef struct ccm_userdata {
+	unsigned char *msa;       /* N x L row-major, states 0..20 */
+	float *weights;           /* N sequence weights (filled by init_cuda/init_b200) */
+	int ncol;                 /* L */
+	int nrow;                 /* N */
+	int nsingle;              /* 20 L */
+	int nvar;                 /* 20 L + 441 L^2 (unpadded count) */
+	void *extra;              /* backend state (a ccm_context*) */
+	float lambda_single;
+	float lambda_pair;
+	float reweighting_threshold;
+	void *meta_steps;
+} ccm_userdata;
+
+/* ---------------------------------------------------------------- sizes */
+CCM_API long long ccm_nsingle_padded(int ncol);
+CCM_API long long ccm_nvar_padded(int ncol);
+
+/* ---------------------------------------------------------------- context API */
+CCM_API void ccm_options_default(ccm_options *opt, int ncol);
+
+/* Upload the alignment and weights, allocate all device state for `path`.
+ * weights == NULL means uniform weights 1.0 (src/reweighting.c:61-67).
+ * Replaces init_cuda (src/evaluate_cuda.c:77-139) without process globals. */
+CCM_API int ccm_create(ccm_context **ctx, const unsigned char *msa, int ncol, int nrow,
+               const float *weights, const ccm_options *opt);
+CCM_API int ccm_destroy(ccm_context *ctx);
+
+/* f and g at x; x and g are DEVICE pointers of nvar_padded floats (the
+ * conjugrad_gpu convention, src/evaluate_cuda.c:23-74).  g is overwritten.
+ * Blocks until the result is on the host; *fx receives f in FP64. */
+CCM_API int ccm_evaluate(ccm_context *ctx, const float *d_x, float *d_g, long long nvar_padded,
+                 double *fx);
+
+/* Same, enqueued on the context stream without a host synchronisation; the
+ * result stays on the device (ccm_result_device) for device-side consumers. */
+CCM_API int ccm_evaluate_async(ccm_context *ctx, const float *d_x, float *d_g, long long nvar_padded);
+
+/* Same with HOST x and g (the evaluate_cpu convention, src/evaluate_cpu.c:16-166):
+ * copies x in, evaluates, copies g out. */
+CCM_API int ccm_evaluate_host(ccm_context *ctx, const float *x, float *g, long long nvar_padded,
+                      double *fx);
+
+/* FP64 evaluation (CCM_PATH_SIMT_F64 contexts): double x and g on the device. */
+CCM_API int ccm_evaluate_f64(ccm_context *ctx, const double *d_x, double *d_g, long long nvar_padded,
+                     double *fx);
+
+/* Device pointer to the ccm_result written by the last evaluation. */
+CCM_API const ccm_result *ccm_result_device(const ccm_context *ctx);
+/* Copy the last ccm_result to the host (synchronises the context stream). */
+CCM_API int ccm_get_result(ccm_context *ctx, ccm_result *out);
+
+/* Sequence weights held by the context (N floats, host). */
+CCM_API int ccm_get_weights(const ccm_context *ctx, float *w);
+
+/* The stream the context runs on (cudaStream_t). */
+CCM_API void *ccm_stream(const ccm_context *ctx);
+
+/* Identity-threshold sequence reweighting on the GPU, bit-exact with the
+ * serial reference calculate_weights (src/reweighting.c:9-58): integer
+ * identity counts, idthres = (int)ceil(threshold * (float)ncol),
+ * w_i = (float)(1.0 / (count_i - 1)) with self counted twice. */
+CCM_API int ccm_calculate_weights(const unsigned char *msa, int ncol, int nrow, float threshold,
+                          float *w, int device);
+
+/* Diagnostics for tests: copy an internal device buffer of a tensor-core
+ * context to host memory `dst` (`bytes` long).  which = 0: one-hot O
+ * (Npad x S bf16); 1..3: Wperm split terms (S x S bf16); 4..6: R split terms
+ * (Npad x S bf16); 7: single-field data gradient (20 L float).  With dst ==
+ * NULL returns the buffer size in bytes; otherwise 0 or a negative status. */
+CCM_API long long ccm_debug_copy(ccm_context *ctx, int which, void *dst, long long bytes);
+
+/* Description of the last error on this host thread. */
+CCM_API const char *ccm_last_error(void);
+
+/* Path used by init_cuda/init_b200 (CCM_PATH_*); default CCM_PATH_TC_BF16X2. */
+CCM_API void ccm_set_default_path(int path);
+
+/* ---------------------------------------------------------------- host-side drop-in pieces */
+/* Bit-identical restatements (float, same operation order) of the reference's
+ * host code around the evaluation. */
+
+/* src/ccmpred.c:90-131 init_bias: x = 0 except V(j,a) = log f_a - log f_gap with
+ * pseudocount 1; x holds nvar_padded floats. */
+CCM_API void ccm_init_bias(const unsigned char *msa, int ncol, int nrow, float *x);
+/* src/util.c:16-64 sum_submatrices (L x L map); returns the coupling norm the
+ * reference prints as "xnorm". */
+CCM_API double ccm_sum_submatrices(const float *x, float *out, int ncol);
+/* src/util.c:66-108 apc, in place. */
+CCM_API void ccm_apc(float *mat, int ncol);
+/* src/util.c:110-140 normalize, in place; CCM_ERR_INVALID on a constant map. */
+CCM_API int ccm_normalize(float *mat, int ncol);
+/* src/io.c:20-28 write_matrix ("%.20e\t"). */
+CCM_API int ccm_write_matrix(const char *path, const float *mat, int ncol, int nrow);
+/* src/io.c:31-60 write_raw. */
+CCM_API int ccm_write_raw(const char *path, const float *x, int ncol);
+/* src/io.c:62-103 read_raw (fills both symmetric halves; x not cleared). */
+CCM_API int ccm_read_raw(const char *path, float *x, int ncol);
+/* src/sequence.c:48-80 read_msa (PSICOV); NULL with *ncol = -1 for a3m/FASTA
+ * input.  Free the result with ccm_free. */
+CCM_API unsigned char *ccm_read_msa(const char *path, int *ncol, int *nrow);
+CCM_API void ccm_free(void *p);
+
+/* ---------------------------------------------------------------- reference triple */
+/* Drop-in for include/evaluate_cuda.h:8-17: device x and g, nvar = nvar_padded,
+ * returns f (src/evaluate_cuda.c:23-74).  init_cuda computes the weights on the
+ * GPU (threshold < 1) or uses uniform weights (src/evaluate_cuda.c:105-125) and,
+ * unlike the reference, also fills ud->weights on the host. */
+CCM_API float evaluate_cuda(void *instance, const float *x, float *g, const int nvar);
+CCM_API int init_cuda(void *instance);
+CCM_API int destroy_cuda(void *instance);
+
+/* Host-pointer backend with the shape of include/evaluate_cpu.h:21-30. */
+CCM_API float evaluate_b200(void *instance, const float *x, float *g, const int nvar);
+CCM_API int init_b200(void *instance);
+CCM_API int destroy_b200(void *instance);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CCMPRED_B200_H */

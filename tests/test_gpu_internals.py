@@ -1,0 +1,108 @@
+"""Stage-by-stage checks of the tensor-core path on small shapes: the one-hot
+operand, the bf16 split of W in the slot layout, the forward GEMM + softmax
+epilogue (through R) and the symmetric backward GEMM (through g), each
+against a float64 numpy restatement of the same stage."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from ccmpred_b200 import Evaluator, lib, synth
+
+pytestmark = pytest.mark.gpu
+
+Q, QP, G = 21, 32, 12
+
+
+def slot(q, l):
+    return (l // G) * 256 + q * G + (l % G)
+
+
+def bf16_to_f32(u16):
+    return (u16.astype(np.uint32) << 16).view(np.float32)
+
+
+def fetch(ev, which, dtype=np.uint16):
+    size = lib().ccm_debug_copy(ev.handle, which, None, 0)
+    assert size > 0
+    buf = np.empty(size // np.dtype(dtype).itemsize, dtype=dtype)
+    assert lib().ccm_debug_copy(ev.handle, which, buf.ctypes.data, size) == 0
+    return buf
+
+
+def expected_internals(msa, w, x, L, lam2):
+    N = msa.shape[0]
+    T = (L + G - 1) // G
+    S = T * 256
+    Npad = (N + 127) // 128 * 128
+    nsp = 20 * L + 32 - (20 * L) % 32
+    V = x[:20 * L].reshape(20, L).astype(np.float64)
+    W = x[nsp:].reshape(Q, L, QP, L)[:, :, :Q, :].astype(np.float64)      # [b,k,a,j]
+    O = np.zeros((Npad, S))
+    for n in range(N):
+        for l in range(L):
+            O[n, slot(msa[n, l], l)] = 1.0
+        O[n, 252] = 1.0
+    Wp = np.zeros((S, S))
+    sl = np.array([[slot(q, l) for l in range(L)] for q in range(Q)])   # [q,l]
+    Wp[np.ix_(sl.reshape(-1), sl.reshape(-1))] = W.reshape(Q * L, Q * L)
+    return O, Wp, V, sl, S, Npad
+
+
+@pytest.mark.parametrize("path", ["tc_bf16x2", "tc_bf16x3"])
+@pytest.mark.parametrize("L,N,seed", [(13, 50, 1), (24, 130, 2), (5, 7, 3)])
+def test_tc_stages(gpu, path, L, N, seed):
+    import torch
+    msa = synth.generate(synth.MSAConfig("t", L, N, n_pairs=2, seed=seed))
+    w = np.random.default_rng(seed).uniform(0.2, 1.0, N).astype(np.float32)
+    x = synth.random_x(L, seed + 10, w_sd=0.05)
+    lam2 = 0.2 * (L - 1)
+    ev = Evaluator(msa, weights=w, lambda_pair=lam2, path=path)
+    xd = torch.from_numpy(x).cuda()
+    gd = torch.empty_like(xd)
+    ev.evaluate(xd, gd)
+    O, Wp, V, sl, S, Npad = expected_internals(msa, w, x, L, lam2)
+    nsplit = 3 if path == "tc_bf16x3" else 2
+
+    # one-hot operand, exact
+    O_gpu = bf16_to_f32(fetch(ev, 0)).reshape(Npad, S)
+    assert np.array_equal(O_gpu, O.astype(np.float32))
+
+    # split terms of W: their sum reproduces W to the split's precision
+    terms = [bf16_to_f32(fetch(ev, 1 + i)).reshape(S, S).astype(np.float64) for i in range(nsplit)]
+    Wsum = sum(terms)
+    tol = 2.0 ** (-16 if nsplit == 2 else -24)
+    assert np.all(np.abs(Wsum - Wp) <= tol * np.abs(Wp) + 1e-30)
+
+    # forward: logits from the split terms, softmax per (row, column), R
+    logits = O[:N] @ Wsum                                   # [n, slot_out]
+    R_exp = np.zeros((Npad, S))
+    for l in range(L):
+        cols = sl[:, l]
+        z = logits[:, cols].copy()
+        z[:, :20] += V[:, l][None, :]
+        z -= z.max(axis=1, keepdims=True)
+        P = np.exp(z) / np.exp(z).sum(axis=1, keepdims=True)
+        onehot = (msa[:, l][:, None] == np.arange(Q)[None, :]).astype(np.float64)
+        R_exp[:N, cols] = w[:, None] * (P - onehot)
+    R_gpu = sum(bf16_to_f32(fetch(ev, 4 + i)).reshape(Npad, S).astype(np.float64)
+                for i in range(nsplit))
+    assert np.abs(R_gpu - R_exp).max() < 1e-5
+
+    # backward: C = O^T R + R^T O from the GPU's own R, compared on g2
+    C = O.T @ R_gpu + R_gpu.T @ O
+    nsp = 20 * L + 32 - (20 * L) % 32
+    g2 = gd.cpu().numpy()[nsp:].reshape(Q, L, QP, L).astype(np.float64)
+    x2 = x[nsp:].reshape(Q, L, QP, L).astype(np.float64)
+    G2 = C[np.ix_(sl.reshape(-1), sl.reshape(-1))].reshape(Q, L, Q, L)
+    idx = np.arange(L)
+    G2[:, idx, :, idx] = 0.0
+    exp_g2 = 2 * np.float32(lam2) * x2.copy()
+    exp_g2[:, :, :Q, :] += G2
+    err = np.abs(g2 - exp_g2).max() / np.abs(exp_g2).max()
+    assert err < 1e-5
+    # single-field data gradient = column sums of R (ones slot of C)
+    g1d = fetch(ev, 7, np.float32).reshape(20, L).astype(np.float64)
+    g1_exp = R_gpu[:, sl[:20].reshape(-1)].sum(axis=0).reshape(20, L)
+    assert np.abs(g1d - g1_exp).max() <= 1e-5 * max(1.0, np.abs(g1_exp).max())
+    ev.close()
