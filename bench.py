@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Benchmark: pseudo-likelihood + gradient evaluations per second at L=300, N=5000.
+
+One step = one evaluation of f and the full gradient at a fixed parameter
+vector x (the reference's evaluate callback, src/evaluate_cuda.c:23-74),
+through the C ABI of libccmpred_b200.so.
+
+  value       evals/s of the split-bf16 tensor-core path with x and g resident
+              in HBM (ccm_evaluate_async back to back, CUDA events on the
+              context stream, max over ranks);
+  e2e         evals/s through the host-pointer C ABI (ccm_evaluate_host):
+              every step copies x host->device from pinned memory and g + f
+              device->host;
+  roofline    the dominant tcgen05 GEMM kernel, algorithmic FLOPs per launch
+              (2 N (21 L)^2, counted once: no hi/lo doubling, no padding) over
+              its CUDA-event time inside the timed region;
+  plain_f32   the same metric on the plain FP32 CUDA-core path (no tensor cores);
+  precision   errors of f and g against the FP64 oracle at the same x;
+  cpu_baseline the reference's evaluate_cpu_omp (compiled from its sources)
+              on a bounded sample, on this host's cores.
+
+`--impl reference` times the reference's own CPU implementation
+(evaluate_cpu_omp, all host threads) on the same workload instead.
+Multi-GPU (torchrun): replicas only -- every rank evaluates its own copy of
+the workload; no data-path collective exists for a single alignment.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PLL+grad evals/s at L=300 N=5000: split-BF16 TC vs plain FP32, rel err≤1e-5"
+UNIT = "evals/s"
+WORKLOAD = "L300_N5000"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=1000)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--path", default="tc_bf16x2", choices=["tc_bf16x2", "tc_bf16x3"])
+    p.add_argument("--e2e-steps", type=int, default=50)
+    p.add_argument("--plain-steps", type=int, default=20)
+    p.add_argument("--cpu-budget-s", type=float, default=15.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-precision", action="store_true")
+    return p.parse_args()
+
+
+def workload():
+    from ccmpred_b200 import synth
+    cfg = synth.PRECISION_300x5000
+    msa = synth.generate(cfg)
+    x = synth.random_x(cfg.ncol, seed=cfg.seed + 1000)
+    return cfg, msa, x
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index)], stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.tmp.flush()
+        self.tmp.seek(0)
+        rows = [r.strip().split(",") for r in self.tmp.read().splitlines() if r.strip()]
+        os.unlink(self.tmp.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [c.strip() for c in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, r[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value: float) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference_timing(msa, x, budget_s, max_evals):
+    """Reference evaluate_cpu_omp (all host threads): (evals/s, evaluations, kind, cores)."""
+    from oracle import oracle as O
+    N, L = msa.shape
+    cores = os.cpu_count() or 1
+    if O.ref_available():
+        ev = O.RefEvaluator(msa, 0.01, 0.2 * (L - 1), 0.8, omp=True)
+        times = []
+        t_start = time.perf_counter()
+        try:
+            for _ in range(max_evals):
+                t0 = time.perf_counter()
+                ev.evaluate(x)
+                times.append(time.perf_counter() - t0)
+                if time.perf_counter() - t_start > budget_s:
+                    break
+        finally:
+            ev.close()
+        return 1.0 / float(np.median(times)), len(times), "reference", cores
+    w = O.oracle_weights(msa, 0.8)
+    times = []
+    t_start = time.perf_counter()
+    for _ in range(max_evals):
+        t0 = time.perf_counter()
+        O.oracle_evaluate(msa, w, 0.01, 0.2 * (L - 1), x)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > budget_s:
+            break
+    return 1.0 / float(np.median(times)), len(times), "port", cores
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    cfg, msa, x = workload()
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libccmref.so (reference CPU sources) was not built"}))
+        return
+    N, L = msa.shape
+    ev = O.RefEvaluator(msa, 0.01, 0.2 * (L - 1), 0.8, omp=True)
+    for _ in range(args.warmup):
+        ev.evaluate(x)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ev.evaluate(x)
+    el = time.perf_counter() - t0
+    ev.close()
+    value = args.steps / el
+    cores = os.cpu_count() or 1
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "ncol": L, "nrow": N, "impl_detail":
+                   "reference evaluate_cpu_omp.c compiled from its sources (-O3 -fopenmp), "
+                   "all host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{args.steps} full evaluations at L=300 N=5000"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def precision_block(msa, w, x, g_gpu, f_gpu, L):
+    from ccmpred_b200 import nsingle_padded
+    from oracle import oracle as O
+    f64, g64 = O.oracle_evaluate(msa, w, 0.01, 0.2 * (L - 1), x)
+    d = g_gpu.astype(np.float64) - g64
+    nsp, ns = nsingle_padded(L), 20 * L
+    n = np.linalg.norm
+    return {"f_rel": abs(f_gpu - f64) / abs(f64), "g_rel": float(n(d) / n(g64)),
+            "g1_rel": float(n(d[:ns]) / n(g64[:ns])), "g2_rel": float(n(d[nsp:]) / n(g64[nsp:])),
+            "reference": "FP64 oracle (oracle/ccm_oracle.c) at the same x and weights"}
+
+
+def traffic_from_profiles(kernel: str):
+    path = os.path.join(ROOT, "profiles", "tc_kernels_L300_N5000.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    k = d.get("kernels", {}).get(kernel)
+    return None if k is None else k.get("dram_bytes_per_launch")
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_init(args)
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        barrier(world)
+        return
+
+    import torch
+
+    import ccmpred_b200 as cb
+    from ccmpred_b200 import _lib
+
+    torch.cuda.set_device(local)
+    cfg, msa, x = workload()
+    N, L = msa.shape
+    t0 = time.perf_counter()
+    w = cb.calculate_weights(msa, 0.8, device=local)
+    init_ms = (time.perf_counter() - t0) * 1e3
+
+    ev = cb.Evaluator(msa, weights=w, path=args.path, device=local)
+    xd = torch.from_numpy(x).cuda()
+    gd = torch.empty_like(xd)
+    stream = torch.cuda.ExternalStream(ev.stream, device=torch.device("cuda", local))
+    for _ in range(max(args.warmup, 3)):
+        ev.evaluate(xd, gd)
+    torch.cuda.synchronize()
+
+    lib = _lib.lib()
+    sampler = ClockSampler(local)
+    launches0 = lib.ccm_launch_count(ev.handle)
+    _lib.check(lib.ccm_profile_begin(ev.handle, args.steps))
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        _lib.check(lib.ccm_evaluate_async(ev.handle, xd.data_ptr(), gd.data_ptr(), xd.numel()))
+    end.record(stream)
+    end.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier(world)
+    elapsed_ms = start.elapsed_time(end)
+    launches = lib.ccm_launch_count(ev.handle) - launches0
+    import ctypes
+    kms = (ctypes.c_double * 8)()
+    nk, ne = ctypes.c_int(0), ctypes.c_int(0)
+    _lib.check(lib.ccm_profile_end(ev.handle, kms, 8, ctypes.byref(nk), ctypes.byref(ne)))
+    names = ["tc_prep", "tc_forward", "tc_backward", "tc_finalize"]
+    kernels = {names[i]: kms[i] / max(ne.value, 1) for i in range(min(nk.value, 4))}
+    elapsed_ms = max_over_ranks(world, elapsed_ms)
+    value = world * args.steps / (elapsed_ms / 1e3)
+    res = ev.result()
+    f_gpu = res.fx
+    g_gpu = gd.cpu().numpy()
+
+    # end to end through the host-pointer ABI (pinned host buffers)
+    xh = torch.from_numpy(x.copy()).pin_memory()
+    gh = torch.empty_like(xh).pin_memory()
+    fx = ctypes.c_double(0.0)
+    xp = ctypes.cast(xh.data_ptr(), ctypes.POINTER(ctypes.c_float))
+    gp = ctypes.cast(gh.data_ptr(), ctypes.POINTER(ctypes.c_float))
+    for _ in range(2):
+        _lib.check(lib.ccm_evaluate_host(ev.handle, xp, gp, xh.numel(), ctypes.byref(fx)))
+    barrier(world)
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for _ in range(args.e2e_steps):
+        _lib.check(lib.ccm_evaluate_host(ev.handle, xp, gp, xh.numel(), ctypes.byref(fx)))
+    e_end.record(stream)
+    e_end.synchronize()
+    e2e_ms = max_over_ranks(world, e_start.elapsed_time(e_end))
+    e2e_value = world * args.e2e_steps / (e2e_ms / 1e3)
+    nbytes = 4 * xh.numel()
+    ev.close()
+
+    out = None
+    if rank == 0:
+        peaks, peak_kind = measured_peaks()
+        peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
+        flops = 2.0 * N * (21 * L) ** 2
+        dom = max(("tc_forward", "tc_backward"), key=lambda k: kernels.get(k, 0.0))
+        dom_ms = kernels.get(dom, float("nan"))
+        achieved = flops / (dom_ms / 1e3) / 1e12
+        traffic = traffic_from_profiles(dom)
+
+        plain = None
+        if args.plain_steps > 0 and world == 1:
+            pe = cb.Evaluator(msa, weights=w, path="simt_f32", device=local)
+            g2 = torch.empty_like(xd)
+            pe.evaluate(xd, g2)
+            torch.cuda.synchronize()
+            ps = torch.cuda.ExternalStream(pe.stream)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(ps)
+            for _ in range(args.plain_steps):
+                _lib.check(lib.ccm_evaluate_async(pe.handle, xd.data_ptr(), g2.data_ptr(), xd.numel()))
+            b.record(ps)
+            b.synchronize()
+            pv = args.plain_steps / (a.elapsed_time(b) / 1e3)
+            f_plain = pe.result().fx
+            g_plain = g2.cpu().numpy()
+            pe.close()
+            plain = {"evals_per_s": pv, "tc_over_plain": value / pv,
+                     "path": "plain FP32 CUDA-core kernels (ccm_simt.cu)"}
+        prec = None
+        if not args.no_precision:
+            prec = {args.path: precision_block(msa, w, x, g_gpu, f_gpu, L)}
+            if plain is not None:
+                prec["simt_f32"] = precision_block(msa, w, x, g_plain, f_plain, L)
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            v, n_ev, kind, cores = cpu_reference_timing(msa, x, args.cpu_budget_s, 10)
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+                   "sample": f"{n_ev} full evaluation(s) of the L=300 N=5000 workload "
+                             f"(median), evaluate_cpu_omp with all {cores} host threads"}
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "ncol": L, "nrow": N, "planted_pairs": cfg.n_pairs,
+                       "seed": cfg.seed, "path": args.path,
+                       "arithmetic": "bf16 hi+lo split operands, f32 tensor-core accumulation, "
+                                     "f64 loss/regulariser reductions",
+                       "l2": "inputs larger than L2 (x and g 242 MB each, bf16 W terms 164 MB)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "tensor", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "peak_source": f"{peak_kind} bf16_tflops_sustained",
+                         "flops_per_launch": flops, "traffic": traffic},
+            "kernels_ms_per_launch": kernels,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes + 32},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "plain_f32": plain,
+            "precision": prec,
+            "init_ms": {"weights": init_ms},
+        }
+        print(json.dumps(out))
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

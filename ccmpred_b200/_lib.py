@@ -70,6 +70,10 @@ SIGNATURES = {
                                              _f32p, ctypes.c_int]),
     "ccm_last_error": (ctypes.c_char_p, []),
     "ccm_debug_copy": (ctypes.c_longlong, [_vp, ctypes.c_int, _vp, ctypes.c_longlong]),
+    "ccm_profile_begin": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "ccm_profile_end": (ctypes.c_int, [_vp, _f64p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)]),
+    "ccm_launch_count": (ctypes.c_longlong, [_vp]),
     "ccm_set_default_path": (None, [ctypes.c_int]),
     "ccm_init_bias": (None, [_u8p, ctypes.c_int, ctypes.c_int, _f32p]),
     "ccm_sum_submatrices": (ctypes.c_double, [_f32p, _f32p, ctypes.c_int]),

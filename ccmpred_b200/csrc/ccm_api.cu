@@ -13,6 +13,15 @@
 #include "ccm_layout.cuh"
 
 namespace ccm {
+
+void prof_mark(ccm_context *c) {
+  if (!c->prof_on || c->prof_eval >= c->prof_max || c->prof_idx >= kMaxProfMarks) return;
+  cudaEventRecord(c->prof_events[c->prof_eval * kMaxProfMarks + c->prof_idx], c->stream);
+  c->prof_idx++;
+}
+
+void count_launch(ccm_context *c, int n) { c->launches += n; }
+
 cudaError_t simt_configure_kernels();
 size_t simt_scratch_bytes(int L, int N, size_t elem);
 cudaError_t reweight_weights(const int *d_counts, float *d_w, int N, cudaStream_t stream);
@@ -169,6 +178,10 @@ void free_all(ccm_context *c) {
   f(c->d_xh); f(c->d_gh);
   if (c->h_out) cudaFreeHost(c->h_out);
   std::free(c->h_w);
+  if (c->prof_events) {
+    for (int i = 0; i < c->prof_max * kMaxProfMarks; ++i) cudaEventDestroy(c->prof_events[i]);
+    std::free(c->prof_events);
+  }
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -182,6 +195,7 @@ int check_status(ccm_context *c) {
 
 int enqueue_eval(ccm_context *c, const float *d_x, float *d_g) {
   CCM_CUDA_TRY(cudaMemsetAsync(c->d_out, 0, sizeof(ccm_result), c->stream));
+  c->prof_idx = 0;
   cudaError_t e;
   switch (c->path) {
     case CCM_PATH_TC_BF16X2:
@@ -193,7 +207,21 @@ int enqueue_eval(ccm_context *c, const float *d_x, float *d_g) {
   }
   if (e != cudaSuccess)
     return set_error(CCM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+  if (c->prof_on && c->prof_eval < c->prof_max) {
+    c->prof_marks_used = c->prof_idx;
+    c->prof_eval++;
+  }
   return CCM_OK;
+}
+
+void free_prof(ccm_context *c) {
+  if (c->prof_events) {
+    for (int i = 0; i < c->prof_max * kMaxProfMarks; ++i) cudaEventDestroy(c->prof_events[i]);
+    std::free(c->prof_events);
+  }
+  c->prof_events = nullptr;
+  c->prof_on = false;
+  c->prof_max = c->prof_eval = 0;
 }
 
 ccm_userdata *as_ud(void *instance) { return static_cast<ccm_userdata *>(instance); }
@@ -407,6 +435,38 @@ long long ccm_debug_copy(ccm_context *c, int which, void *dst, long long bytes) 
   CCM_CUDA_TRY(cudaMemcpy(dst, src, (size_t)size, cudaMemcpyDeviceToHost));
   return CCM_OK;
 }
+
+int ccm_profile_begin(ccm_context *c, int max_evals) {
+  if (!c || max_evals <= 0) return set_error(CCM_ERR_INVALID, "ccm_profile_begin: invalid arguments");
+  free_prof(c);
+  c->prof_events = static_cast<cudaEvent_t *>(std::calloc((size_t)max_evals * kMaxProfMarks, sizeof(cudaEvent_t)));
+  if (!c->prof_events) return set_error(CCM_ERR_NOMEM, "ccm_profile_begin: host allocation");
+  c->prof_max = max_evals;
+  for (int i = 0; i < max_evals * kMaxProfMarks; ++i) CCM_CUDA_TRY(cudaEventCreate(&c->prof_events[i]));
+  c->prof_eval = 0;
+  c->prof_on = true;
+  return CCM_OK;
+}
+
+int ccm_profile_end(ccm_context *c, double *kernel_ms, int max_kernels, int *n_kernels, int *n_evals) {
+  if (!c || !c->prof_on) return set_error(CCM_ERR_INVALID, "ccm_profile_end: profiling not active");
+  CCM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const int nk = c->prof_marks_used > 0 ? c->prof_marks_used - 1 : 0;
+  for (int k = 0; k < max_kernels; ++k) kernel_ms[k] = 0.0;
+  for (int e = 0; e < c->prof_eval; ++e)
+    for (int k = 0; k < nk && k < max_kernels; ++k) {
+      float ms = 0.0f;
+      CCM_CUDA_TRY(cudaEventElapsedTime(&ms, c->prof_events[e * kMaxProfMarks + k],
+                                        c->prof_events[e * kMaxProfMarks + k + 1]));
+      kernel_ms[k] += ms;
+    }
+  if (n_kernels) *n_kernels = nk;
+  if (n_evals) *n_evals = c->prof_eval;
+  free_prof(c);
+  return CCM_OK;
+}
+
+long long ccm_launch_count(const ccm_context *c) { return c ? c->launches : -1; }
 
 const ccm_result *ccm_result_device(const ccm_context *c) { return c ? c->d_out : nullptr; }
 

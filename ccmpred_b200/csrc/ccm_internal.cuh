@@ -65,6 +65,12 @@ struct FinalizeArgs {
   ccm_result *out;
 };
 
+// Per-kernel CUDA-event timing of evaluations (ccm_profile_begin/end): one
+// event before the first kernel of an evaluation and one after each kernel.
+constexpr int kMaxProfMarks = 8;
+void prof_mark(ccm_context *c);
+void count_launch(ccm_context *c, int n = 1);
+
 cudaError_t tc_configure_kernels();
 cudaError_t tc_evaluate(ccm_context *c, const float *d_x, float *d_g);
 int tc_fwd_smem_bytes(int nsplit);
@@ -118,4 +124,10 @@ struct ccm_context {
 
   // host-pointer evaluation scratch
   float *d_xh = nullptr, *d_gh = nullptr;
+
+  // instrumentation
+  long long launches = 0;              // kernels launched by this context
+  bool prof_on = false;
+  int prof_max = 0, prof_eval = 0, prof_idx = 0, prof_marks_used = 0;
+  cudaEvent_t *prof_events = nullptr;  // prof_max * kMaxProfMarks
 };

@@ -213,20 +213,27 @@ static cudaError_t simt_run(ccm_context *c, const T *d_x, T *d_g) {
   int threads = ((L + 31) / 32) * 32;
   if (threads > 256) threads = 256;
   const int grid_rows = N < 65535 ? N : 65535;
+  prof_mark(c);
   simt_rows_kernel<T><<<grid_rows, threads, L, c->stream>>>(c->d_msa, c->d_w, x1, x2, R, part_f, L, N);
 
   const size_t pair_smem = sizeof(T) * kPairK * kQ * kPairCols;
   dim3 pgrid((unsigned)((QL + kPairCols - 1) / kPairCols), (unsigned)((L + kPairK - 1) / kPairK));
+  prof_mark(c);
   simt_pairs_kernel<T><<<pgrid, kPairCols, pair_smem, c->stream>>>(c->d_msa, R, G2, L, N);
+  prof_mark(c);
 
   const int nsingle = (kQ - 1) * L;
   simt_single_kernel<T><<<(nsingle + 127) / 128, 128, 0, c->stream>>>(R, g1d, L, N);
+  prof_mark(c);
 
   simt_sym_kernel<T><<<kQ * L, 256, 0, c->stream>>>(G2, x2, g2, part_reg, L, (T)c->lambda_pair);
+  prof_mark(c);
 
   simt_finalize_kernel<T><<<1, 1024, 0, c->stream>>>(part_f, N, part_reg, kQ * L, x1, g1d, g1,
                                                      c->nsp, L, (T)c->lambda_single,
                                                      (T)c->lambda_pair, c->d_out);
+  prof_mark(c);
+  count_launch(c, 5);
   return cudaGetLastError();
 }
 

@@ -634,7 +634,9 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
   PrepArgs pa{};
   pa.L = L; pa.S = c->S; pa.lambda_pair = c->lambda_pair; pa.part_reg = c->d_part_reg;
   for (int i = 0; i < 3; ++i) pa.wperm[i] = c->d_wperm[i];
+  prof_mark(c);
   tc_prep_kernel<NSPLIT><<<kQ * L, 256, 0, c->stream>>>(x2, g2, pa);
+  prof_mark(c);
 
   FwdArgs fa{};
   fa.msa = c->d_msa; fa.w = c->d_w; fa.x1 = x1; fa.part_f = c->d_part_f; fa.status = c->d_status;
@@ -644,6 +646,7 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
   const int fwd_grid = fwd_tiles < c->num_sms ? fwd_tiles : c->num_sms;
   tc_forward_kernel<NSPLIT><<<fwd_grid, kThreads, FwdSmem<NSPLIT>::kTotal, c->stream>>>(
       c->fwd_maps, fa);
+  prof_mark(c);
 
   BwdArgs ba{};
   ba.x2 = x2; ba.g2 = g2; ba.g1d = c->d_g1d; ba.tiles = c->d_bwd_tiles;
@@ -652,6 +655,7 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
   const int bwd_grid = c->n_bwd_tiles < c->num_sms ? c->n_bwd_tiles : c->num_sms;
   tc_backward_kernel<NSPLIT><<<bwd_grid, kThreads, BwdSmem<NSPLIT>::kTotal, c->stream>>>(
       c->bwd_maps, ba);
+  prof_mark(c);
 
   FinalizeArgs za{};
   za.part_f = c->d_part_f; za.n_part_f = (long long)fwd_tiles * 4;
@@ -659,6 +663,8 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
   za.x1 = x1; za.g1d = c->d_g1d; za.g1 = d_g; za.L = L; za.nsp = c->nsp;
   za.lambda_single = c->lambda_single; za.lambda_pair = c->lambda_pair; za.out = c->d_out;
   tc_finalize_kernel<<<1, 1024, 0, c->stream>>>(za);
+  prof_mark(c);
+  count_launch(c, 4);
   return cudaGetLastError();
 }
 

@@ -145,6 +145,18 @@ CCM_API void *ccm_stream(const ccm_context *ctx);
 CCM_API int ccm_calculate_weights(const unsigned char *msa, int ncol, int nrow, float threshold,
                           float *w, int device);
 
+/* Instrumentation.  ccm_profile_begin records CUDA events on the context
+ * stream around every kernel of the next max_evals evaluations;
+ * ccm_profile_end synchronises and returns, per kernel position in the
+ * launch sequence, the summed device time in ms (tensor-core path: prep,
+ * forward, backward, finalize; SIMT path: rows, pairs, single, sym,
+ * finalize), the number of kernels per evaluation and of evaluations seen. */
+CCM_API int ccm_profile_begin(ccm_context *ctx, int max_evals);
+CCM_API int ccm_profile_end(ccm_context *ctx, double *kernel_ms, int max_kernels, int *n_kernels,
+                            int *n_evals);
+/* Number of kernels this context has launched (evaluations only). */
+CCM_API long long ccm_launch_count(const ccm_context *ctx);
+
 /* Diagnostics for tests: copy an internal device buffer of a tensor-core
  * context to host memory `dst` (`bytes` long).  which = 0: one-hot O
  * (Npad x S bf16); 1..3: Wperm split terms (S x S bf16); 4..6: R split terms

@@ -41,7 +41,7 @@ def expected_internals(msa, w, x, L, lam2):
     O = np.zeros((Npad, S))
     for n in range(N):
         for l in range(L):
-            O[n, slot(msa[n, l], l)] = 1.0
+            O[n, slot(int(msa[n, l]), l)] = 1.0
         O[n, 252] = 1.0
     Wp = np.zeros((S, S))
     sl = np.array([[slot(q, l) for l in range(L)] for q in range(Q)])   # [q,l]

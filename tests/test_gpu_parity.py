@@ -15,12 +15,18 @@ from ccmpred_b200 import Evaluator, _lib, calculate_weights, lib, nsingle_padded
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
-# relative error bounds vs FP64 (f, g1, g2).  The FP32 reference itself is
-# within ~2e-6 of FP64 at these sizes (tests/test_oracle.py).
+# Error bounds vs the FP64 oracle at identical x, per result:
+#   f      relative error of f;
+#   g      relative L2 error of the whole gradient (the headline bound, 1e-5);
+#   g1, g2 L2 error of the single-field / coupling part divided by the L2 norm
+#          of the whole gradient.  At x0 = init_bias the single-field gradient
+#          nearly cancels (sum_n w P ~ sum_n w onehot), so its error relative
+#          to its own norm is large for every FP32 evaluator, the reference's
+#          evaluate_cpu included (1.2e-3 at L=300, N=5000).
 TOL = {
-    "simt_f32": (1e-5, 1e-5, 1e-5),
-    "tc_bf16x2": (1e-5, 1e-5, 1e-5),
-    "tc_bf16x3": (1e-5, 1e-5, 1e-5),
+    "simt_f32": dict(f=1e-6, g=1e-5, g1=1e-5, g2=1e-5),
+    "tc_bf16x2": dict(f=1e-6, g=1e-5, g1=1e-5, g2=1e-5),
+    "tc_bf16x3": dict(f=1e-6, g=1e-5, g1=1e-5, g2=1e-5),
 }
 PATHS = list(TOL)
 
@@ -28,12 +34,14 @@ PATHS = list(TOL)
 def errors(f, g, f64, g64, L):
     nsp = nsingle_padded(L)
     ns = 20 * L
+    d = g.astype(np.float64) - g64
+    gn = max(np.linalg.norm(g64), 1e-300)
+    return dict(f=abs(f - f64) / abs(f64), g=float(np.linalg.norm(d) / gn),
+                g1=float(np.linalg.norm(d[:ns]) / gn), g2=float(np.linalg.norm(d[nsp:]) / gn))
 
-    def rel(a, b):
-        return float(np.linalg.norm(a.astype(np.float64) - b) / max(np.linalg.norm(b), 1e-300))
 
-    return (abs(f - f64) / abs(f64), rel(g[:ns], g64[:ns]), rel(g[nsp:], g64[nsp:]),
-            float(np.abs(g.astype(np.float64) - g64).max() / np.abs(g64).max()))
+def within(e, tol, slack=0.0):
+    return all(e[k] < tol[k] + slack for k in tol)
 
 
 def run(path, msa, w, x, lam1, lam2):
@@ -56,12 +64,11 @@ def test_golden(gpu, oracle_mod, path, fixture):
     f, g = run(path, msa, w, x, lam1, lam2)
     assert np.all(np.isfinite(g))
     f64, g64 = oracle_mod.oracle_evaluate(msa, w, lam1, lam2, x)
-    ef, e1, e2, _ = errors(f, g, f64, g64, msa.shape[1])
-    tf, t1, t2 = TOL[path]
-    assert ef < tf and e1 < t1 and e2 < t2, (ef, e1, e2)
-    # against the reference's own FP32 output
-    ef_r, e1_r, e2_r, _ = errors(f, g, float(d["f"]), d["g"].astype(np.float64), msa.shape[1])
-    assert ef_r < tf + 2e-6 and e1_r < t1 + 2e-6 and e2_r < t2 + 2e-6
+    e = errors(f, g, f64, g64, msa.shape[1])
+    assert within(e, TOL[path]), e
+    # against the reference's own FP32 output (its error vs FP64 is ~1e-6 here)
+    e_ref = errors(f, g, float(d["f"]), d["g"].astype(np.float64), msa.shape[1])
+    assert within(e_ref, TOL[path], slack=2e-6), e_ref
 
 
 CASES = [
@@ -87,9 +94,8 @@ def test_synthetic(gpu, oracle_mod, path, name, cfg, xkind):
         x = synth.random_x(L, cfg.seed + 7)
     f, g = run(path, msa, w, x, lam1, lam2)
     f64, g64 = oracle_mod.oracle_evaluate(msa, w, lam1, lam2, x)
-    ef, e1, e2, _ = errors(f, g, f64, g64, L)
-    tf, t1, t2 = TOL[path]
-    assert ef < tf and e1 < t1 and e2 < t2, (ef, e1, e2)
+    e = errors(f, g, f64, g64, L)
+    assert within(e, TOL[path]), e
 
 
 @pytest.mark.parametrize("path", ["tc_bf16x2", "simt_f32"])
@@ -102,8 +108,8 @@ def test_inadmissible_x(gpu, oracle_mod, path):
     w = np.ones(40, np.float32)
     f, g = run(path, msa, w, x, 0.01, 2.0)
     f64, g64 = oracle_mod.oracle_evaluate(msa, w, 0.01, 2.0, x)
-    ef, e1, e2, _ = errors(f, g, f64, g64, L)
-    assert ef < 1e-5 and e1 < 1e-5 and e2 < 1e-5, (ef, e1, e2)
+    e = errors(f, g, f64, g64, L)
+    assert within(e, TOL[path]), e
 
 
 def test_weights_bit_exact(gpu, oracle_mod):
@@ -137,8 +143,8 @@ def test_reference_triple(gpu, oracle_mod):
     gd = torch.empty_like(xd)
     f = lib().evaluate_cuda(ctypes.byref(ud), xd.data_ptr(), gd.data_ptr(), x.size)
     f64, g64 = oracle_mod.oracle_evaluate(msa, wbuf, 0.01, 0.2 * (L - 1), x)
-    ef, e1, e2, _ = errors(f, gd.cpu().numpy(), f64, g64, L)
-    assert ef < 1e-5 and e1 < 1e-5 and e2 < 1e-5
+    e = errors(f, gd.cpu().numpy(), f64, g64, L)
+    assert within(e, TOL["tc_bf16x2"]), e
     # host-pointer variant on a second instance
     ud2 = _lib.CcmUserdata.from_buffer_copy(ud)
     ud2.extra = None
@@ -157,10 +163,8 @@ def test_errors_and_determinism(gpu):
     ev = Evaluator(msa)
     x = torch.from_numpy(synth.random_x(30, 1)).cuda()
     g = torch.empty_like(x)
-    with pytest.raises(_lib.CcmError) as e:
-        lib().ccm_evaluate(ev.handle, x.data_ptr(), g.data_ptr(), x.numel() - 1, None) and \
-            _lib.check(lib().ccm_evaluate(ev.handle, x.data_ptr(), g.data_ptr(), x.numel() - 1, None))
-        raise _lib.CcmError(-1, "unreachable")
+    rc = lib().ccm_evaluate(ev.handle, x.data_ptr(), g.data_ptr(), x.numel() - 1, None)
+    assert rc == _lib.CCM_ERR_INVALID and b"nvar" in lib().ccm_last_error()
     f1 = ev.evaluate(x, g)
     g1 = g.clone()
     f2 = ev.evaluate(x, g)
