@@ -23,45 +23,86 @@
 namespace ccm {
 
 // ------------------------------------------------------------------ tc_prep
-// One block per row (b,k) of the reference W matrix.  Reads that row (32 L
-// floats), writes the bf16 split terms of its 21 L real entries to row s(b,k)
-// of every Wperm_i at columns s(a,j), writes g2 = 2*lambda2*x on the padding
-// states a in [21,32), and leaves one FP64 partial of sum x^2 per row.
+// One block per row (b,k) of the reference W matrix.  The row's 21 L real
+// entries are staged in shared memory (coalesced float4 loads); every thread
+// then emits 8 consecutive slots of row s(b,k) of each Wperm_i as one 16-byte
+// store (padding slots written as 0).  The whole g2 row is initialised to the
+// regulariser gradient 2*lambda2*x (src/evaluate_cpu.c:158-161); tc_backward
+// later adds the data term with one atomic add per element.  One FP64 partial
+// of sum x^2 per row (all 32 L slots).
 template <int NSPLIT>
 __global__ void __launch_bounds__(256) tc_prep_kernel(const float *__restrict__ x2,
                                                       float *__restrict__ g2, PrepArgs args) {
+  extern __shared__ __align__(16) float xrow[];  // 21 L floats
   const int L = args.L;
-  const int row = blockIdx.x;           // b*L + k
+  const int row = blockIdx.x;  // b*L + k
   const int b = row / L, k = row % L;
   const long long base = (long long)row * kQPad * L;
-  const long long srow = (long long)slot_of(b, k) * args.S;
   const float two_l2 = 2.0f * args.lambda_pair;
+  const int nreal = kQ * L;
   double acc = 0.0;
-  for (int a = 0; a < kQPad; ++a) {
-    const float *xr = x2 + base + (long long)a * L;
-    if (a < kQ) {
-      for (int j = threadIdx.x; j < L; j += blockDim.x) {
-        const float v = xr[j];
-        acc += (double)v * (double)v;
-        const long long dst = srow + slot_of(a, j);
-        const __nv_bfloat16 h = __float2bfloat16_rn(v);
-        const float r1 = v - __bfloat162float(h);
-        const __nv_bfloat16 l1 = __float2bfloat16_rn(r1);
-        args.wperm[0][dst] = h;
-        args.wperm[1][dst] = l1;
-        if (NSPLIT > 2) {
-          const float r2 = r1 - __bfloat162float(l1);
-          args.wperm[2][dst] = __float2bfloat16_rn(r2);
-        }
-      }
-    } else {
-      float *gr = g2 + base + (long long)a * L;
-      for (int j = threadIdx.x; j < L; j += blockDim.x) {
-        const float v = xr[j];
-        acc += (double)v * (double)v;
-        gr[j] = two_l2 * v;
-      }
+  // rows start at a multiple of 32 L floats (16-byte aligned); L % 4 == 0 allows float4
+  if ((L & 3) == 0) {
+    const float4 *src = reinterpret_cast<const float4 *>(x2 + base);
+    float4 *dst = reinterpret_cast<float4 *>(g2 + base);
+    for (int i = threadIdx.x; i < nreal / 4; i += blockDim.x) {
+      const float4 v = src[i];
+      acc += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w;
+      reinterpret_cast<float4 *>(xrow)[i] = v;
+      dst[i] = make_float4(two_l2 * v.x, two_l2 * v.y, two_l2 * v.z, two_l2 * v.w);
     }
+    const float4 *srcp = reinterpret_cast<const float4 *>(x2 + base + nreal);
+    float4 *dstp = reinterpret_cast<float4 *>(g2 + base + nreal);
+    for (int i = threadIdx.x; i < (kQPad - kQ) * L / 4; i += blockDim.x) {
+      const float4 v = srcp[i];
+      acc += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w;
+      dstp[i] = make_float4(two_l2 * v.x, two_l2 * v.y, two_l2 * v.z, two_l2 * v.w);
+    }
+  } else {
+    for (int i = threadIdx.x; i < nreal; i += blockDim.x) {
+      const float v = x2[base + i];
+      acc += (double)v * v;
+      xrow[i] = v;
+      g2[base + i] = two_l2 * v;
+    }
+    for (int i = nreal + threadIdx.x; i < kQPad * L; i += blockDim.x) {
+      const float v = x2[base + i];
+      acc += (double)v * v;
+      g2[base + i] = two_l2 * v;
+    }
+  }
+  __syncthreads();
+  const long long srow = (long long)slot_of(b, k) * args.S;
+  for (int u = threadIdx.x; u < args.S / 8; u += blockDim.x) {
+    uint32_t p0[4], p1[4], p2[4];
+#pragma unroll
+    for (int e2 = 0; e2 < 4; ++e2) {
+      uint32_t h0 = 0, h1 = 0, h2 = 0;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int sl = u * 8 + e2 * 2 + e;
+        const int t = sl / kGroupSlots, r = sl % kGroupSlots;
+        float v = 0.0f;
+        if (r < kGroupUsed) {
+          const int a = r / kGroupCols, j = t * kGroupCols + r % kGroupCols;
+          if (j < L) v = xrow[a * L + j];
+        }
+        const __nv_bfloat16 hb = __float2bfloat16_rn(v);
+        const float r1 = v - __bfloat162float(hb);
+        const __nv_bfloat16 lb = __float2bfloat16_rn(r1);
+        h0 |= (uint32_t)__bfloat16_as_ushort(hb) << (16 * e);
+        h1 |= (uint32_t)__bfloat16_as_ushort(lb) << (16 * e);
+        if (NSPLIT > 2)
+          h2 |= (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(r1 - __bfloat162float(lb)))
+                << (16 * e);
+      }
+      p0[e2] = h0; p1[e2] = h1; p2[e2] = h2;
+    }
+    const long long off = srow + (long long)u * 8;
+    *reinterpret_cast<uint4 *>(args.wperm[0] + off) = make_uint4(p0[0], p0[1], p0[2], p0[3]);
+    *reinterpret_cast<uint4 *>(args.wperm[1] + off) = make_uint4(p1[0], p1[1], p1[2], p1[3]);
+    if (NSPLIT > 2)
+      *reinterpret_cast<uint4 *>(args.wperm[2] + off) = make_uint4(p2[0], p2[1], p2[2], p2[3]);
   }
   // block reduction, fixed order
   __shared__ double red[32];
@@ -69,9 +110,9 @@ __global__ void __launch_bounds__(256) tc_prep_kernel(const float *__restrict__ 
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
   __syncthreads();
   if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-    args.part_reg[row] = s;
+    double sum = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += red[w];
+    args.part_reg[row] = sum;
   }
 }
 
@@ -383,7 +424,9 @@ struct BwdSmem {
   static constexpr int kOffRQ = kOffOQ + kB;
   static constexpr int kStage = kOffRQ + NSPLIT * kB;
   static constexpr int kBarOff = kStages * kStage;
-  static constexpr int kTotal = kBarOff + 256 + 1024;
+  static constexpr int kTOff = kBarOff + 256;                    // epilogue transpose buffers
+  static constexpr int kTBytes = 4 * 32 * 17 * 4;                // 4 warps x 32 rows x 16(+1) cols
+  static constexpr int kTotal = kTOff + kTBytes + 1024;
 };
 
 template <int NSPLIT>
@@ -510,23 +553,32 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (!mbar_wait(drain, 0)) record_error(args.status, kErrBwdTimeout, abort_flag);
     }
   } else {
+    // Epilogue.  Element (s1, s2), s1 <= s2, of the symmetric C goes to
+    //   direct      g2 row (b,k) = s1, column (a,j) = s2
+    //   transposed  g2 row (a,j) = s2, column (b,k) = s1   (s1 != s2)
+    // Transposed writes are issued thread-major (consecutive lanes = consecutive
+    // k: contiguous runs).  Direct writes go through a per-warp shared-memory
+    // transpose so that one warp instruction covers 2 rows x 16 columns, i.e.
+    // runs of consecutive j, instead of 32 different rows.
+    // g2 already holds 2*lambda2*x (tc_prep); every element receives exactly
+    // one atomic add of its C value (none on self-edge blocks), so the result
+    // does not depend on the order of the adds.
     const int q = warp & 3;
     const int L = args.L;
-    const float two_l2 = 2.0f * args.lambda_pair;
-    const float *__restrict__ x2 = args.x2;
     float *__restrict__ g2 = args.g2;
+    float *Tb = reinterpret_cast<float *>(smem + SM::kTOff) + (warp - 2) * 32 * 17;
     int local = 0;
     for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++local) {
       if (__shfl_sync(0xffffffffu, aborted(abort_flag) ? 1 : 0, 0)) break;
       const int acc = local & 1;
       const uint32_t use = local >> 1;
       const int2 pq = args.tiles[tile];
-      const int s1 = pq.x * kBwdBM + q * 32 + lane;
+      const int rowbase = pq.x * kBwdBM + q * 32;
+      const int s1 = rowbase + lane;
       const int t1 = s1 / kGroupSlots, r1 = s1 % kGroupSlots;
       const int b = r1 / kGroupCols, k = t1 * kGroupCols + r1 % kGroupCols;
       const bool valid1 = r1 < kGroupUsed && k < L;
-      const long long rowd = valid1 ? x2_index(b, k, 0, 0, L) : 0;  // + a*L + j
-      const long long colt = (long long)b * L + k;                  // + ((a*L+j)*32)*L
+      const long long colt = (long long)b * L + k;  // transposed: + ((a*L+j)*32)*L
       const int sQ = pq.y * kBwdBN;
       const int jQ = pq.y * kGroupCols;
 
@@ -543,6 +595,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         __syncwarp();
         tmem_ld32(taddr + c * 32, v);
         tmem_wait_ld();
+        // (A) transposed writes and the ones-slot column, thread-major
 #pragma unroll
         for (int i = 0; i < 32; ++i) {
           const int r2 = c * 32 + i;
@@ -550,19 +603,38 @@ __global__ void __launch_bounds__(kThreads, 1)
           const int a = r2 / kGroupCols, j = jQ + r2 % kGroupCols;
           const bool valid2 = r2 < kGroupUsed && j < L;
           const float cval = __uint_as_float(v[i]);
-          if (s1 <= s2) {
+          if (s1 < s2) {
             if (valid1 && valid2) {
-              const float gd = (k == j) ? 0.0f : cval;
-              const long long id = rowd + (long long)a * L + j;
-              g2[id] = gd + two_l2 * x2[id];
-              if (s1 != s2) {
-                const long long it2 = ((long long)a * L + j) * kQPad * L + colt;
-                g2[it2] = gd + two_l2 * x2[it2];
-              }
-            } else if (s1 == kOnesSlot && valid2 && a < kQ - 1) {
-              args.g1d[a * L + j] = cval;
+              if (k != j) atomicAdd(g2 + ((long long)a * L + j) * kQPad * L + colt, cval);
             } else if (s2 == kOnesSlot && valid1 && b < kQ - 1) {
               args.g1d[b * L + k] = cval;
+            }
+          }
+        }
+        // (B) direct writes and the ones-slot row, through the transpose buffer
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          __syncwarp();
+#pragma unroll
+          for (int e = 0; e < 16; ++e) Tb[lane * 17 + e] = __uint_as_float(v[h * 16 + e]);
+          __syncwarp();
+          const int col = lane & 15;
+          const int r2 = c * 32 + h * 16 + col;
+          const int s2 = sQ + r2;
+          const int a = r2 / kGroupCols, j = jQ + r2 % kGroupCols;
+          const bool valid2 = r2 < kGroupUsed && j < L;
+#pragma unroll 4
+          for (int it = 0; it < 16; ++it) {
+            const int row = 2 * it + (lane >> 4);
+            const int s1r = rowbase + row;
+            if (s1r > s2) continue;
+            const float val = Tb[row * 17 + col];
+            const int tr = s1r / kGroupSlots, rr = s1r % kGroupSlots;
+            const int br = rr / kGroupCols, kr = tr * kGroupCols + rr % kGroupCols;
+            if (rr < kGroupUsed && kr < L) {
+              if (valid2 && kr != j) atomicAdd(g2 + x2_index(br, kr, a, j, L), val);
+            } else if (s1r == kOnesSlot && valid2 && a < kQ - 1) {
+              args.g1d[a * L + j] = val;
             }
           }
         }
@@ -635,7 +707,7 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
   pa.L = L; pa.S = c->S; pa.lambda_pair = c->lambda_pair; pa.part_reg = c->d_part_reg;
   for (int i = 0; i < 3; ++i) pa.wperm[i] = c->d_wperm[i];
   prof_mark(c);
-  tc_prep_kernel<NSPLIT><<<kQ * L, 256, 0, c->stream>>>(x2, g2, pa);
+  tc_prep_kernel<NSPLIT><<<kQ * L, 256, sizeof(float) * kQ * L, c->stream>>>(x2, g2, pa);
   prof_mark(c);
 
   FwdArgs fa{};
@@ -670,6 +742,11 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
 
 cudaError_t tc_configure_kernels() {
   cudaError_t e;
+  // the staged W row is 21 L floats: up to L = 2000 (168 KB)
+  e = cudaFuncSetAttribute(tc_prep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 168000);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(tc_prep_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 168000);
+  if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(tc_forward_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            FwdSmem<2>::kTotal);
   if (e != cudaSuccess) return e;
