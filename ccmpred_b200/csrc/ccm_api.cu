@@ -69,9 +69,12 @@ EncodeTiledFn get_encode_fn() {
   return fn;
 }
 
-// 2-D bf16 row-major [rows][cols] tensor, 128B-swizzled boxes of box_cols x box_rows.
+// 2-D bf16 row-major [rows][cols] tensor, swizzled boxes of box_cols x box_rows
+// (128-byte swizzle for 64-column boxes, 64-byte swizzle for 32-column boxes).
 int make_map_bf16(CUtensorMap *map, void *base, long long rows, long long cols, int box_cols,
                   int box_rows) {
+  const CUtensorMapSwizzle swz =
+      box_cols * 2 == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
   EncodeTiledFn enc = get_encode_fn();
   if (!enc) return set_error(CCM_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
   cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
@@ -79,7 +82,7 @@ int make_map_bf16(CUtensorMap *map, void *base, long long rows, long long cols, 
   cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return set_error(CCM_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return CCM_OK;
@@ -130,7 +133,7 @@ int alloc_tc(ccm_context *c) {
     CCM_CUDA_TRY(cudaMemsetAsync(c->d_r[i], 0, sizeof(__nv_bfloat16) * Np * S, c->stream));
   }
   const long long fwd_tiles = (long long)(c->Npad / 128) * c->T;
-  CCM_CUDA_TRY(cudaMalloc(&c->d_part_f, sizeof(double) * fwd_tiles * 4));
+  CCM_CUDA_TRY(cudaMalloc(&c->d_part_f, sizeof(double) * fwd_tiles * 8));
   CCM_CUDA_TRY(cudaMalloc(&c->d_part_reg, sizeof(double) * kQ * c->L));
   CCM_CUDA_TRY(cudaMalloc(&c->d_g1d, sizeof(float) * (kQ - 1) * c->L));
 
@@ -151,10 +154,10 @@ int alloc_tc(ccm_context *c) {
   std::memset(&c->fwd_maps, 0, sizeof(c->fwd_maps));
   std::memset(&c->bwd_maps, 0, sizeof(c->bwd_maps));
   int rc;
-  if ((rc = make_map_bf16(&c->fwd_maps.a, c->d_onehot, Np, S, 64, 128)) != CCM_OK) return rc;
+  if ((rc = make_map_bf16(&c->fwd_maps.a, c->d_onehot, Np, S, 32, 128)) != CCM_OK) return rc;
   if ((rc = make_map_bf16(&c->bwd_maps.o, c->d_onehot, Np, S, 64, 32)) != CCM_OK) return rc;
   for (int i = 0; i < c->nsplit; ++i) {
-    if ((rc = make_map_bf16(&c->fwd_maps.b[i], c->d_wperm[i], S, S, 64, 64)) != CCM_OK) return rc;
+    if ((rc = make_map_bf16(&c->fwd_maps.b[i], c->d_wperm[i], S, S, 64, 32)) != CCM_OK) return rc;
     if ((rc = make_map_bf16(&c->bwd_maps.r[i], c->d_r[i], Np, S, 64, 32)) != CCM_OK) return rc;
   }
   return CCM_OK;

@@ -15,8 +15,8 @@ constexpr int kErrFwdTimeout = 1;
 constexpr int kErrBwdTimeout = 2;
 
 struct FwdMaps {
-  CUtensorMap a;      // one-hot O [Npad][S], box 64 (slots, K) x 128 (rows)
-  CUtensorMap b[3];   // Wperm_i  [S][S],   box 64 (out slots, N) x 64 (in slots, K)
+  CUtensorMap a;      // one-hot O [Npad][S], box 32 (slots, K) x 128 (rows), 64B swizzle
+  CUtensorMap b[3];   // Wperm_i  [S][S],   box 64 (out slots, N) x 32 (in slots, K)
 };
 
 struct BwdMaps {

@@ -117,18 +117,24 @@ __global__ void __launch_bounds__(256) tc_prep_kernel(const float *__restrict__ 
 }
 
 // --------------------------------------------------------------- tc_forward
-constexpr int kFwdBM = 128, kFwdBN = 256, kFwdBK = 64;
-constexpr int kFwdStages = 2;
-constexpr int kThreads = 192;  // warp 0: TMA, warp 1: MMA, warps 2-5: epilogue
+constexpr int kFwdBM = 128, kFwdBN = 256, kFwdBK = 32;
+// forward: warp 0 TMA, warp 1 MMA, warps 2-9 epilogue (two warps per TMEM lane
+// quarter, each owning half of the 256 accumulator columns)
+constexpr int kFwdThreads = 320;
+// backward: warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int kThreads = 192;
 
 template <int NSPLIT>
 struct FwdSmem {
-  static constexpr int kABytes = kFwdBM * kFwdBK * 2;            // 16 KB
-  static constexpr int kBBytes = kFwdBN * kFwdBK * 2;            // 32 KB per term
+  static constexpr int kStages = NSPLIT == 2 ? 5 : 3;
+  static constexpr int kABytes = kFwdBM * kFwdBK * 2;            // 8 KB, K-major, 64B swizzle
+  static constexpr int kBBytes = kFwdBN * kFwdBK * 2;            // 16 KB per term, MN-major
   static constexpr int kStage = kABytes + NSPLIT * kBBytes;
-  static constexpr int kBarOff = kFwdStages * kStage;
-  static constexpr int kVOff = kBarOff + 256;
-  static constexpr int kTotal = kVOff + 240 * 4 + 1024;            // + alignment slack
+  static constexpr int kBarOff = kStages * kStage;
+  static constexpr int kVOff = kBarOff + 256;                     // V of the tile's 12 columns
+  static constexpr int kXOff = kVOff + 1024;                       // half-to-half exchange
+  static constexpr int kXBytes = 2 * kFwdBM * 12 * 4;              // [half][row][12]
+  static constexpr int kTotal = kXOff + kXBytes + 1024;            // + alignment slack
 };
 
 __device__ __forceinline__ uint8_t *align1024(uint8_t *p) {
@@ -145,10 +151,142 @@ __device__ __forceinline__ bool aborted(const int *abort_flag) {
   return *reinterpret_cast<const volatile int *>(abort_flag) != 0;
 }
 
+// Forward epilogue for one warp: TMEM lane quarter q, column half H (chunks
+// 4H..4H+3 of the 8 x 32 accumulator columns).  The softmax over the 21
+// states of each of the 12 alignment columns of the tile needs both halves:
+// the per-column max and sum of exp are exchanged with the partner warp
+// (same rows, other half) through shared memory.
+template <int NSPLIT, int H>
+__device__ __forceinline__ void fwd_epilogue_tile(const FwdArgs &args, uint32_t taddr, const float *Vs,
+                                                  float *xbuf, int q, int lane, int n, int t,
+                                                  long long tile) {
+  const int L = args.L;
+  const int j0 = t * kGroupCols;
+  const bool live = n < args.N;
+  const float wn = live ? args.w[n] : 0.0f;
+  const int row = q * 32 + lane;
+  const int pair_bar = 2 + q;
+  int xr[kGroupCols];
+#pragma unroll
+  for (int jj = 0; jj < kGroupCols; ++jj) {
+    const int j = j0 + jj;
+    xr[jj] = (live && j < L) ? (int)args.msa[(long long)n * L + j] : -1;
+  }
+  const volatile float *Vv = Vs;
+  float *mine = xbuf + (H * kFwdBM + row) * kGroupCols;
+  const float *other = xbuf + ((1 - H) * kFwdBM + row) * kGroupCols;
+
+  float mx[kGroupCols], tg[kGroupCols], se[kGroupCols];
+#pragma unroll
+  for (int jj = 0; jj < kGroupCols; ++jj) { mx[jj] = -INFINITY; tg[jj] = 0.0f; se[jj] = 0.0f; }
+  // pass A: max over own states, logit of the observed state if it is ours
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    uint32_t v[32];
+    __syncwarp();
+    tmem_ld32(taddr + (4 * H + c) * 32, v);
+    tmem_wait_ld();
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      const int col = (4 * H + c) * 32 + i;
+      if (col < kGroupUsed) {
+        const int a = col / kGroupCols, jj = col % kGroupCols;
+        const float z = __uint_as_float(v[i]) + (a < kQ - 1 ? Vv[a * kGroupCols + jj] : 0.0f);
+        mx[jj] = fmaxf(mx[jj], z);
+        if (xr[jj] == a) tg[jj] = z;
+      }
+    }
+  }
+#pragma unroll
+  for (int jj = 0; jj < kGroupCols; ++jj) mine[jj] = mx[jj];
+  named_bar_sync(pair_bar, 64);
+#pragma unroll
+  for (int jj = 0; jj < kGroupCols; ++jj) mx[jj] = fmaxf(mx[jj], other[jj]);
+  named_bar_sync(pair_bar, 64);  // partner has read `mine`
+  // pass B: own part of the sum of exp
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    uint32_t v[32];
+    __syncwarp();
+    tmem_ld32(taddr + (4 * H + c) * 32, v);
+    tmem_wait_ld();
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      const int col = (4 * H + c) * 32 + i;
+      if (col < kGroupUsed) {
+        const int a = col / kGroupCols, jj = col % kGroupCols;
+        const float z = __uint_as_float(v[i]) + (a < kQ - 1 ? Vv[a * kGroupCols + jj] : 0.0f);
+        se[jj] += expf(z - mx[jj]);
+      }
+    }
+  }
+#pragma unroll
+  for (int jj = 0; jj < kGroupCols; ++jj) mine[jj] = se[jj];
+  named_bar_sync(pair_bar, 64);
+  float lse[kGroupCols];
+  double floss = 0.0;
+#pragma unroll
+  for (int jj = 0; jj < kGroupCols; ++jj) {
+    // both halves form the same sum: H=0 adds (own + partner), H=1 (partner + own)
+    const float tot = H == 0 ? se[jj] + other[jj] : other[jj] + se[jj];
+    lse[jj] = mx[jj] + logf(tot);
+    // the loss term belongs to the half holding the observed state's column
+    if (xr[jj] >= 0 && ((xr[jj] * kGroupCols + jj) >> 7) == H)
+      floss += (double)(wn * (lse[jj] - tg[jj]));
+  }
+  // pass C: R = w (P - onehot) over own 128 slots, split into bf16 terms
+  const long long rbase = (long long)n * args.S + (long long)t * kGroupSlots;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int cc = 4 * H + c;
+    uint32_t v[32];
+    __syncwarp();
+    tmem_ld32(taddr + cc * 32, v);
+    tmem_wait_ld();
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      uint32_t ph[4], pl[4], pl2[4];
+#pragma unroll
+      for (int e2 = 0; e2 < 4; ++e2) {
+        uint32_t hh = 0, ll = 0, l2 = 0;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int i = u * 8 + e2 * 2 + e;
+          const int col = cc * 32 + i;
+          float r = 0.0f;
+          if (col < kGroupUsed) {
+            const int a = col / kGroupCols, jj = col % kGroupCols;
+            const float z = __uint_as_float(v[i]) + (a < kQ - 1 ? Vv[a * kGroupCols + jj] : 0.0f);
+            if (xr[jj] >= 0) r = wn * (expf(z - lse[jj]) - (xr[jj] == a ? 1.0f : 0.0f));
+          }
+          const __nv_bfloat16 hb = __float2bfloat16_rn(r);
+          const float rr = r - __bfloat162float(hb);
+          const __nv_bfloat16 lb = __float2bfloat16_rn(rr);
+          hh |= (uint32_t)__bfloat16_as_ushort(hb) << (16 * e);
+          ll |= (uint32_t)__bfloat16_as_ushort(lb) << (16 * e);
+          if (NSPLIT > 2)
+            l2 |= (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(rr - __bfloat162float(lb)))
+                  << (16 * e);
+        }
+        ph[e2] = hh; pl[e2] = ll; pl2[e2] = l2;
+      }
+      const long long off = rbase + cc * 32 + u * 8;
+      *reinterpret_cast<uint4 *>(args.r[0] + off) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+      *reinterpret_cast<uint4 *>(args.r[1] + off) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+      if (NSPLIT > 2)
+        *reinterpret_cast<uint4 *>(args.r[2] + off) = make_uint4(pl2[0], pl2[1], pl2[2], pl2[3]);
+    }
+  }
+  // loss partial, one per (tile, epilogue warp), summed in fixed order by tc_finalize
+  for (int o = 16; o > 0; o >>= 1) floss += __shfl_xor_sync(0xffffffffu, floss, o);
+  if (lane == 0) args.part_f[tile * 8 + H * 4 + q] = floss;
+}
+
 template <int NSPLIT>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kFwdThreads, 1)
     tc_forward_kernel(const __grid_constant__ FwdMaps maps, FwdArgs args) {
   using SM = FwdSmem<NSPLIT>;
+  constexpr int kFwdStages = SM::kStages;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = align1024(smem_raw);
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + SM::kBarOff);
@@ -159,6 +297,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
   int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
   float *Vs = reinterpret_cast<float *>(smem + SM::kVOff);
+  float *xbuf = reinterpret_cast<float *>(smem + SM::kXOff);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n_tiles = args.m_tiles * args.T;
@@ -166,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kFwdStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
-    for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 4); }
+    for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 8); }
     mbar_init(drain, 1);
     *abort_flag = 0;
     fence_mbar_init();
@@ -243,7 +382,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           const uint32_t b0 = a0 + SM::kABytes;
 #pragma unroll
           for (int k16 = 0; k16 < kFwdBK / 16; ++k16) {
-            const uint64_t ad = sdesc_sw128(a0 + k16 * 32, 16, 1024);
+            const uint64_t ad = sdesc_sw64(a0 + k16 * 32, 16, 512);
 #pragma unroll
             for (int i = 0; i < NSPLIT; ++i) {
               const uint64_t bd =
@@ -260,142 +399,44 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (!mbar_wait(drain, 0)) record_error(args.status, kErrFwdTimeout, abort_flag);
     }
   } else {
-    // ---------------- epilogue: 4 warps, warp w owns TMEM lanes 32*(w%4) ...
+    // ---------------- epilogue: 8 warps; warp w owns TMEM lanes 32*(w%4) ...
+    // and column half (w-2)/4
     const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
     const int ethr = threadIdx.x - 64;
     const int L = args.L;
     int local = 0;
     for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++local) {
-      // all four epilogue warps agree here: every one finished the previous
+      // all eight epilogue warps agree here: every one finished the previous
       // tile (so Vs may be overwritten) and none has seen an abort
-      if (named_bar_or(1, 128, aborted(abort_flag))) break;
+      if (named_bar_or(1, 256, aborted(abort_flag))) break;
       const int acc = local & 1;
       const uint32_t use = local >> 1;
       const int m = tile % args.m_tiles, t = tile / args.m_tiles;
       const int j0 = t * kGroupCols;
-      for (int idx = ethr; idx < (kQ - 1) * kGroupCols; idx += 128) {
-        const int a = idx / kGroupCols, j = j0 + idx % kGroupCols;
-        Vs[idx] = (j < L) ? args.x1[a * L + j] : 0.0f;
+      if (ethr < (kQ - 1) * kGroupCols) {
+        const int a = ethr / kGroupCols, j = j0 + ethr % kGroupCols;
+        Vs[ethr] = (j < L) ? args.x1[a * L + j] : 0.0f;
       }
-      named_bar_sync(1, 128);
-
+      named_bar_sync(1, 256);
       const int n = m * kFwdBM + q * 32 + lane;
-      const bool live = n < args.N;
-      const float wn = live ? args.w[n] : 0.0f;
-      int xr[kGroupCols];
-#pragma unroll
-      for (int jj = 0; jj < kGroupCols; ++jj) {
-        const int j = j0 + jj;
-        xr[jj] = (live && j < L) ? (int)args.msa[(long long)n * L + j] : -1;
-      }
       bool ok = mbar_wait(&tfull[acc], use & 1);
       if (__any_sync(0xffffffffu, !ok)) {
-        // leave through the agreement barrier at the top of the loop
+        // leave through the agreement barrier at the top of the loop; the
+        // partner warp times out on the same barrier
         if (lane == 0) record_error(args.status, kErrFwdTimeout, abort_flag);
         continue;
       }
       tc_fence_after();
       const uint32_t taddr = tmem_base + acc * kFwdBN + ((uint32_t)(q * 32) << 16);
-      // volatile: re-read V from shared memory in every pass instead of keeping
-      // 240 values live in registers across the three passes
-      const volatile float *Vv = Vs;
-
-      float mx[kGroupCols], tg[kGroupCols], se[kGroupCols];
-#pragma unroll
-      for (int jj = 0; jj < kGroupCols; ++jj) { mx[jj] = -INFINITY; tg[jj] = 0.0f; se[jj] = 0.0f; }
-
-      // pass A: max over states, logit of the observed state
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        uint32_t v[32];
-        __syncwarp();
-        tmem_ld32(taddr + c * 32, v);
-        tmem_wait_ld();
-#pragma unroll
-        for (int i = 0; i < 32; ++i) {
-          const int col = c * 32 + i;
-          if (col < kGroupUsed) {
-            const int a = col / kGroupCols, jj = col % kGroupCols;
-            const float z = __uint_as_float(v[i]) + (a < kQ - 1 ? Vv[a * kGroupCols + jj] : 0.0f);
-            mx[jj] = fmaxf(mx[jj], z);
-            if (xr[jj] == a) tg[jj] = z;
-          }
-        }
-      }
-      // pass B: sum of exp
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        uint32_t v[32];
-        __syncwarp();
-        tmem_ld32(taddr + c * 32, v);
-        tmem_wait_ld();
-#pragma unroll
-        for (int i = 0; i < 32; ++i) {
-          const int col = c * 32 + i;
-          if (col < kGroupUsed) {
-            const int a = col / kGroupCols, jj = col % kGroupCols;
-            const float z = __uint_as_float(v[i]) + (a < kQ - 1 ? Vv[a * kGroupCols + jj] : 0.0f);
-            se[jj] += expf(z - mx[jj]);
-          }
-        }
-      }
-      float lse[kGroupCols];
-      double floss = 0.0;
-#pragma unroll
-      for (int jj = 0; jj < kGroupCols; ++jj) {
-        lse[jj] = mx[jj] + logf(se[jj]);
-        if (xr[jj] >= 0) floss += (double)(wn * (lse[jj] - tg[jj]));
-      }
-      // pass C: R = w (P - onehot), split into bf16 terms, stored row-major [n][slot]
-      const long long rbase = (long long)n * args.S + (long long)t * kGroupSlots;
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        uint32_t v[32];
-        __syncwarp();
-        tmem_ld32(taddr + c * 32, v);
-        tmem_wait_ld();
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {        // 8 slots -> one 16-byte store per term
-          uint32_t ph[4], pl[4], pl2[4];
-#pragma unroll
-          for (int e2 = 0; e2 < 4; ++e2) {
-            uint32_t hh = 0, ll = 0, l2 = 0;
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-              const int i = u * 8 + e2 * 2 + e;
-              const int col = c * 32 + i;
-              float r = 0.0f;
-              if (col < kGroupUsed) {
-                const int a = col / kGroupCols, jj = col % kGroupCols;
-                const float z =
-                    __uint_as_float(v[i]) + (a < kQ - 1 ? Vv[a * kGroupCols + jj] : 0.0f);
-                if (xr[jj] >= 0) r = wn * (expf(z - lse[jj]) - (xr[jj] == a ? 1.0f : 0.0f));
-              }
-              const __nv_bfloat16 hb = __float2bfloat16_rn(r);
-              const float rr = r - __bfloat162float(hb);
-              const __nv_bfloat16 lb = __float2bfloat16_rn(rr);
-              hh |= (uint32_t)__bfloat16_as_ushort(hb) << (16 * e);
-              ll |= (uint32_t)__bfloat16_as_ushort(lb) << (16 * e);
-              if (NSPLIT > 2)
-                l2 |= (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(rr - __bfloat162float(lb)))
-                      << (16 * e);
-            }
-            ph[e2] = hh; pl[e2] = ll; pl2[e2] = l2;
-          }
-          const long long off = rbase + c * 32 + u * 8;
-          *reinterpret_cast<uint4 *>(args.r[0] + off) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
-          *reinterpret_cast<uint4 *>(args.r[1] + off) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
-          if (NSPLIT > 2)
-            *reinterpret_cast<uint4 *>(args.r[2] + off) = make_uint4(pl2[0], pl2[1], pl2[2], pl2[3]);
-        }
-      }
+      if (half == 0)
+        fwd_epilogue_tile<NSPLIT, 0>(args, taddr, Vs, xbuf, q, lane, n, t, tile);
+      else
+        fwd_epilogue_tile<NSPLIT, 1>(args, taddr, Vs, xbuf, q, lane, n, t, tile);
       // accumulator may be reused by the MMA warp
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&tempty[acc]);
-      // loss partial, one per (tile, warp), summed in fixed order by tc_finalize
-      for (int o = 16; o > 0; o >>= 1) floss += __shfl_xor_sync(0xffffffffu, floss, o);
-      if (lane == 0) args.part_f[(long long)tile * 4 + q] = floss;
     }
   }
 
@@ -716,7 +757,7 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
   fa.L = L; fa.N = c->N; fa.S = c->S; fa.T = c->T; fa.Npad = c->Npad; fa.m_tiles = c->Npad / kFwdBM;
   const int fwd_tiles = fa.m_tiles * c->T;
   const int fwd_grid = fwd_tiles < c->num_sms ? fwd_tiles : c->num_sms;
-  tc_forward_kernel<NSPLIT><<<fwd_grid, kThreads, FwdSmem<NSPLIT>::kTotal, c->stream>>>(
+  tc_forward_kernel<NSPLIT><<<fwd_grid, kFwdThreads, FwdSmem<NSPLIT>::kTotal, c->stream>>>(
       c->fwd_maps, fa);
   prof_mark(c);
 
@@ -730,7 +771,7 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
   prof_mark(c);
 
   FinalizeArgs za{};
-  za.part_f = c->d_part_f; za.n_part_f = (long long)fwd_tiles * 4;
+  za.part_f = c->d_part_f; za.n_part_f = (long long)fwd_tiles * 8;
   za.part_reg = c->d_part_reg; za.n_part_reg = (long long)kQ * L;
   za.x1 = x1; za.g1d = c->d_g1d; za.g1 = d_g; za.L = L; za.nsp = c->nsp;
   za.lambda_single = c->lambda_single; za.lambda_pair = c->lambda_pair; za.out = c->d_out;
