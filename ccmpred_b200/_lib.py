@@ -68,6 +68,8 @@ SIGNATURES = {
     "ccm_stream": (_vp, [_vp]),
     "ccm_calculate_weights": (ctypes.c_int, [_u8p, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                              _f32p, ctypes.c_int]),
+    "ccm_calculate_weights_noalloc": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int,
+                                                     ctypes.c_float, _vp, _vp]),
     "ccm_last_error": (ctypes.c_char_p, []),
     "ccm_debug_copy": (ctypes.c_longlong, [_vp, ctypes.c_int, _vp, ctypes.c_longlong]),
     "ccm_profile_begin": (ctypes.c_int, [_vp, ctypes.c_int]),

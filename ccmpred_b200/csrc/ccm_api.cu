@@ -22,6 +22,8 @@ void prof_mark(ccm_context *c) {
 
 void count_launch(ccm_context *c, int n) { c->launches += n; }
 
+int set_last_error(int code, const char *fmt, ...);
+
 cudaError_t simt_configure_kernels();
 size_t simt_scratch_bytes(int L, int N, size_t elem);
 cudaError_t reweight_weights(const int *d_counts, float *d_w, int N, cudaStream_t stream);
@@ -41,6 +43,18 @@ int set_error(int code, const char *fmt, ...) {
   va_end(ap);
   return code;
 }
+
+}  // namespace
+
+int ccm::set_last_error(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+namespace {
 
 #define CCM_CUDA_TRY(expr)                                                                  \
   do {                                                                                      \

@@ -7,6 +7,9 @@
 // j != i with ids > idthres and +2 for j == i (the reference's i <= j loop
 // visits the diagonal once and increments w[i] twice).  Counts are integers,
 // so the order of the atomic additions does not matter.
+#include <cstdio>
+#include <mutex>
+
 #include <cuda_runtime.h>
 
 #include "ccm_internal.cuh"
@@ -127,3 +130,160 @@ cudaError_t reweight_weights(const int *d_counts, float *d_w, int N, cudaStream_
 }
 
 }  // namespace ccm
+
+// ----------------------------------------------------------------------------
+// Allocation-free variant of the sequence reweighting (ccm_calculate_weights_noalloc).
+//
+// Its only scratch, one identity count per sequence, lives in the file-scope
+// device array below instead of memory obtained from cudaMalloc/cudaMallocAsync,
+// and the count kernel packs the alignment bytes into words in shared memory
+// instead of in a packed copy in global memory.  The array is part of the
+// library image: every GPU that loads the library holds it until the process
+// exits.  All calls share it and it keeps the counts of the last call, so each
+// call clears the part it uses first; calls that overlap on the GPU (different
+// streams, or different host threads on one device) race on it.
+namespace ccm {
+
+constexpr int kNoAllocMaxRows = 262144;  // 1 MiB of int counts
+static __device__ __align__(256) int g_noalloc_counts[kNoAllocMaxRows];
+
+__global__ void __launch_bounds__(256) rw_count_bytes_kernel(const uint8_t *__restrict__ msa,
+                                                             int L, int N, int words, int npad,
+                                                             int idthres, int *__restrict__ counts) {
+  const int IB = blockIdx.y, JB = blockIdx.x;
+  if (JB < IB) return;
+  __shared__ uint32_t As[kRwTile][kRwChunk + 1];
+  __shared__ uint32_t Bs[kRwTile][kRwChunk + 1];
+  __shared__ int ci[kRwTile], cj[kRwTile];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const int i0 = IB * kRwTile, j0 = JB * kRwTile;
+  if (threadIdx.x < kRwTile) { ci[threadIdx.x] = 0; cj[threadIdx.x] = 0; }
+  int ids[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) ids[u][v] = 0;
+
+  for (int w0 = 0; w0 < words; w0 += kRwChunk) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < kRwTile * kRwChunk; e += blockDim.x) {
+      const int r = e / kRwChunk, wd = e % kRwChunk;
+      const int ia = i0 + r, jb = j0 + r, k0 = (w0 + wd) * 4;
+      uint32_t wa = 0, wb = 0;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int k = k0 + b;
+        if (k < L) {
+          if (ia < N) wa |= (uint32_t)msa[(long long)ia * L + k] << (8 * b);
+          if (jb < N) wb |= (uint32_t)msa[(long long)jb * L + k] << (8 * b);
+        }
+      }
+      As[r][wd] = wa;
+      Bs[r][wd] = wb;
+    }
+    __syncthreads();
+    const int wmax = (words - w0) < kRwChunk ? (words - w0) : kRwChunk;
+    for (int wd = 0; wd < wmax; ++wd) {
+      uint32_t a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) a[u] = As[ty * 4 + u][wd];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) b[v] = Bs[tx * 4 + v][wd];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) ids[u][v] += __popc(__vcmpeq4(a[u], b[v]));
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int il = ty * 4 + u, jl = tx * 4 + v;
+      const int i = i0 + il, j = j0 + jl;
+      if (i >= N || j >= N) continue;
+      const int same = ids[u][v] / 8 - npad;
+      if (same <= idthres) continue;
+      if (IB == JB) {
+        if (i < j) { atomicAdd(&ci[il], 1); atomicAdd(&ci[jl], 1); }
+        else if (i == j) atomicAdd(&ci[il], 2);
+      } else {
+        atomicAdd(&ci[il], 1);
+        atomicAdd(&cj[jl], 1);
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kRwTile) {
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.x;
+    if (i < N && ci[threadIdx.x]) atomicAdd(&counts[i], ci[threadIdx.x]);
+    if (IB != JB && j < N && cj[threadIdx.x]) atomicAdd(&counts[j], cj[threadIdx.x]);
+  }
+}
+
+}  // namespace ccm
+
+namespace {
+
+std::mutex g_noalloc_mutex;
+int *g_noalloc_addr[64] = {nullptr};
+
+}  // namespace
+
+// See include/ccmpred_b200.h.  Set-up (first call on a device, under a lock):
+// look up the device address of the count array with cudaGetSymbolAddress
+// while that device is current -- host code must not use the array's name as
+// a device pointer.  After that a call only enqueues a memset and two kernels.
+extern "C" CCM_API int ccm_calculate_weights_noalloc(const unsigned char *d_msa, int ncol,
+                                                     int nrow, float threshold, float *d_w,
+                                                     void *stream) {
+  using namespace ccm;
+  if (!d_msa || !d_w || ncol <= 0 || nrow <= 0) {
+    return set_last_error(CCM_ERR_INVALID, "ccm_calculate_weights_noalloc: invalid arguments");
+  }
+  if (nrow > kNoAllocMaxRows) {
+    return set_last_error(CCM_ERR_INVALID,
+                          "ccm_calculate_weights_noalloc: nrow=%d exceeds the fixed scratch of %d "
+                          "sequences",
+                          nrow, kNoAllocMaxRows);
+  }
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+    return set_last_error(CCM_ERR_CUDA, "ccm_calculate_weights_noalloc: no current device (%s)",
+                          cudaGetErrorString(e));
+  }
+  int *counts;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+      void *p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_noalloc_counts);
+      if (e != cudaSuccess || !p) {
+        return set_last_error(CCM_ERR_CUDA,
+                              "ccm_calculate_weights_noalloc: cudaGetSymbolAddress failed (%s)",
+                              cudaGetErrorString(e));
+      }
+      g_noalloc_addr[dev] = static_cast<int *>(p);
+    }
+    counts = g_noalloc_addr[dev];
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const float prod = threshold * (float)(uint64_t)ncol;  // src/reweighting.c:10
+  const int idthres = (int)ceil((double)prod);
+  const int words = (ncol + 3) / 4;
+  const int npad = words * 4 - ncol;
+  e = cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nrow, s);
+  if (e == cudaSuccess) {
+    const int nb = (nrow + kRwTile - 1) / kRwTile;
+    rw_count_bytes_kernel<<<dim3(nb, nb), 256, 0, s>>>(d_msa, ncol, nrow, words, npad, idthres,
+                                                        counts);
+    rw_weights_kernel<<<(nrow + 255) / 256, 256, 0, s>>>(counts, d_w, nrow);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    return set_last_error(CCM_ERR_CUDA, "ccm_calculate_weights_noalloc: %s", cudaGetErrorString(e));
+  }
+  return CCM_OK;
+}

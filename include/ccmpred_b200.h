@@ -164,6 +164,29 @@ CCM_API long long ccm_launch_count(const ccm_context *ctx);
  * NULL returns the buffer size in bytes; otherwise 0 or a negative status. */
 CCM_API long long ccm_debug_copy(ccm_context *ctx, int which, void *dst, long long bytes);
 
+/* Allocation-free sequence reweighting.  No counterpart in the reference.
+ *
+ * For callers that must not allocate device memory: a process whose memory
+ * pool or framework already owns (nearly) all of the GPU's memory, so that a
+ * cudaMalloc would fail or force the pool to give memory back, or a pipeline
+ * that cannot afford the device-wide synchronisation that cudaFree implies.
+ * Same result as ccm_calculate_weights (bit-exact with the reference's serial
+ * calculate_weights), but with DEVICE pointers: d_msa (nrow x ncol states)
+ * in, d_w (nrow floats) out, enqueued on `stream` (a cudaStream_t, NULL for
+ * the legacy default stream) on the current device, without a host
+ * synchronisation.  It calls no cudaMalloc, cudaFree or other allocating
+ * routine: its only scratch, one int count per sequence, is a fixed array
+ * compiled into the library (1 MiB, nrow <= 262144; larger nrow is rejected
+ * with CCM_ERR_INVALID).  Every GPU that loads the library keeps that array
+ * until the process exits.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress); after that a call only enqueues a
+ * memset and two kernels.  All calls share the array and it keeps the last
+ * call's counts (each call clears what it uses first): calls that overlap on
+ * the GPU race on it and must be serialised by the caller (one stream, or
+ * events between streams). */
+CCM_API int ccm_calculate_weights_noalloc(const unsigned char *d_msa, int ncol, int nrow,
+                                          float threshold, float *d_w, void *stream);
+
 /* Description of the last error on this host thread. */
 CCM_API const char *ccm_last_error(void);
 
