@@ -118,6 +118,27 @@ class Evaluator:
                                      ctypes.byref(fx)))
         return fx.value
 
+    def minimize(self, x, max_iterations: int = 250, epsilon: float = 0.01, k: int = 5,
+                 progress=None, **kw) -> "_lib.CcmCgResult":
+        """Device conjugate gradient from x (a float32 CUDA tensor, updated in place).
+
+        ``progress(k, ls, fx, xnorm, gnorm, step)`` is called after every
+        iteration; returning True stops the run."""
+        p = _lib.CcmCgParams()
+        lib().ccm_cg_params_default(ctypes.byref(p))
+        p.max_iterations, p.epsilon, p.k = max_iterations, epsilon, k
+        for name, val in kw.items():
+            setattr(p, name, val)
+        res = _lib.CcmCgResult()
+        cb = _lib.PROGRESS(0)
+        if progress is not None:
+            def _cb(inst, xp, gp, fx, xnorm, gnorm, step, n, kk, ls):
+                return 1 if progress(kk, ls, fx, xnorm, gnorm, step) else 0
+            cb = _lib.PROGRESS(_cb)
+        check(lib().ccm_conjugrad_gpu(self._ctx, x.data_ptr(), x.numel(), ctypes.byref(p), cb,
+                                      None, ctypes.byref(res)))
+        return res
+
     def evaluate_async(self, x, g) -> None:
         check(lib().ccm_evaluate_async(self._ctx, x.data_ptr(), g.data_ptr(), x.numel()))
 

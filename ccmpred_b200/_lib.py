@@ -46,6 +46,31 @@ class CcmUserdata(ctypes.Structure):
                 ("reweighting_threshold", ctypes.c_float), ("meta_steps", ctypes.c_void_p)]
 
 
+class CcmCgParams(ctypes.Structure):
+    _fields_ = [("max_iterations", ctypes.c_int), ("k", ctypes.c_int),
+                ("max_linesearch", ctypes.c_int), ("pad", ctypes.c_int),
+                ("epsilon", ctypes.c_double), ("alpha_mul", ctypes.c_double),
+                ("ftol", ctypes.c_double), ("wolfe", ctypes.c_double)]
+
+
+class CcmCgResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("iterations", ctypes.c_int),
+                ("evaluations", ctypes.c_int), ("pad", ctypes.c_int),
+                ("fx", ctypes.c_double), ("gnorm", ctypes.c_double)]
+
+
+CG_SUCCESS = 0
+CG_ALREADY_MINIMIZED = 1
+CG_STOPPED = 2
+CG_ERR_MAXITER = -1023
+CG_ERR_LINESEARCH = -1022
+CG_ERR_NONFINITE = -1021
+
+# progress(instance, x, g, fx, xnorm, gnorm, step, n, k, ls) -> int
+PROGRESS = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                            ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                            ctypes.c_int, ctypes.c_int, ctypes.c_int)
+
 # name -> (restype, argtypes); every symbol include/ccmpred_b200.h declares
 _vp = ctypes.c_void_p
 _f32p = ctypes.POINTER(ctypes.c_float)
@@ -77,6 +102,15 @@ SIGNATURES = {
                                        ctypes.POINTER(ctypes.c_int)]),
     "ccm_launch_count": (ctypes.c_longlong, [_vp]),
     "ccm_set_default_path": (None, [ctypes.c_int]),
+    "ccm_cg_params_default": (None, [ctypes.POINTER(CcmCgParams)]),
+    "ccm_conjugrad_gpu": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, ctypes.POINTER(CcmCgParams),
+                                         PROGRESS, _vp, ctypes.POINTER(CcmCgResult)]),
+    "ccm_conjugrad_host": (ctypes.c_int, [_vp, _f32p, ctypes.c_longlong, ctypes.POINTER(CcmCgParams),
+                                          PROGRESS, _vp, ctypes.POINTER(CcmCgResult)]),
+    "ccm_device_count": (ctypes.c_int, []),
+    "ccm_device_info": (ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_size_t),
+                                       ctypes.POINTER(ctypes.c_size_t)]),
     "ccm_init_bias": (None, [_u8p, ctypes.c_int, ctypes.c_int, _f32p]),
     "ccm_sum_submatrices": (ctypes.c_double, [_f32p, _f32p, ctypes.c_int]),
     "ccm_apc": (None, [_f32p, ctypes.c_int]),

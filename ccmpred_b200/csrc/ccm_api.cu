@@ -241,6 +241,14 @@ void free_prof(ccm_context *c) {
   c->prof_max = c->prof_eval = 0;
 }
 
+}  // namespace
+
+int ccm::enqueue_evaluation(ccm_context *c, const float *d_x, float *d_g) {
+  return enqueue_eval(c, d_x, d_g);
+}
+
+namespace {
+
 ccm_userdata *as_ud(void *instance) { return static_cast<ccm_userdata *>(instance); }
 
 [[noreturn]] void die_ref(const char *what) {

@@ -82,6 +82,9 @@ cudaError_t simt_evaluate_f64(ccm_context *c, const double *d_x, double *d_g);
 // Record a message for ccm_last_error() and return `code`.
 int set_last_error(int code, const char *fmt, ...);
 
+// Enqueue one evaluation of the context's path on its stream (no host sync).
+int enqueue_evaluation(ccm_context *c, const float *d_x, float *d_g);
+
 cudaError_t reweight_counts(const uint8_t *d_msa, int L, int N, int idthres, int *d_counts,
                             cudaStream_t stream);
 

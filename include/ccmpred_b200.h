@@ -193,6 +193,62 @@ CCM_API const char *ccm_last_error(void);
 /* Path used by init_cuda/init_b200 (CCM_PATH_*); default CCM_PATH_TC_BF16X2. */
 CCM_API void ccm_set_default_path(int path);
 
+/* ---------------------------------------------------------------- optimizer */
+/* Device-side nonlinear conjugate gradient over a context's evaluation; the
+ * replacement of libconjugrad's conjugrad_gpu (src/ccmpred.c:632-648, absent
+ * from the reference checkout).  Parameters as set at src/ccmpred.c:526-534;
+ * FP64 line-search tests and dot products, float vectors on the device. */
+typedef struct ccm_cg_params {
+	int max_iterations;   /* -n, default 250 (src/ccmpred.c:222) */
+	int k;                /* -k, default 5: convergence window */
+	int max_linesearch;   /* 5 */
+	int pad;
+	double epsilon;       /* -e, default 0.01: stop when (f_{i-k} - f_i)/|f_i| < epsilon */
+	double alpha_mul;     /* 0.5: backtracking factor */
+	double ftol;          /* 1e-4: sufficient-decrease constant */
+	double wolfe;         /* 0.2: curvature constant */
+} ccm_cg_params;
+
+typedef struct ccm_cg_result {
+	int status;       /* CCM_CG_* */
+	int iterations;
+	int evaluations;
+	int pad;
+	double fx;        /* f at the returned x */
+	double gnorm;     /* ||g|| at the returned x */
+} ccm_cg_result;
+
+#define CCM_CG_SUCCESS 0
+#define CCM_CG_ALREADY_MINIMIZED 1
+#define CCM_CG_STOPPED 2
+#define CCM_CG_ERR_MAXITER (-1023)
+#define CCM_CG_ERR_LINESEARCH (-1022)
+#define CCM_CG_ERR_NONFINITE (-1021)
+
+/* Progress callback with the signature of the reference's progress()
+ * (src/ccmpred.c:50-61); x and g are device pointers.  Non-zero stops the run. */
+typedef int (*ccm_progress_t)(void *instance, const float *x, const float *g, const float fx,
+                              const float xnorm, const float gnorm, const float step, int n, int k,
+                              int ls);
+
+CCM_API void ccm_cg_params_default(ccm_cg_params *p);
+/* Minimise f starting from the DEVICE vector d_x (nvar_padded floats, updated
+ * in place).  Returns CCM_OK with the optimizer outcome in *result, or a
+ * CCM_ERR_* status when the device or an argument fails. */
+CCM_API int ccm_conjugrad_gpu(ccm_context *ctx, float *d_x, long long n,
+                              const ccm_cg_params *params, ccm_progress_t progress, void *instance,
+                              ccm_cg_result *result);
+
+/* Same with a HOST x (copied to the device, optimised, copied back). */
+CCM_API int ccm_conjugrad_host(ccm_context *ctx, float *x, long long n,
+                               const ccm_cg_params *params, ccm_progress_t progress,
+                               void *instance, ccm_cg_result *result);
+
+/* Devices (src/ccmpred.c:400-478 device selection and memory report). */
+CCM_API int ccm_device_count(void);
+CCM_API int ccm_device_info(int device, char *name, int name_len, size_t *mem_free,
+                            size_t *mem_total);
+
 /* ---------------------------------------------------------------- host-side drop-in pieces */
 /* Bit-identical restatements (float, same operation order) of the reference's
  * host code around the evaluation. */

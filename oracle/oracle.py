@@ -70,6 +70,14 @@ def oracle_lib():
         lib.oracle_calculate_weights.restype = None
         lib.oracle_calculate_weights.argtypes = [_u8p, ctypes.c_int, ctypes.c_int,
                                                  ctypes.c_float, _f32p]
+        lib.oracle_conjugrad_f64.restype = ctypes.c_int
+        lib.oracle_conjugrad_f64.argtypes = [_u8p, _f64p, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_double, ctypes.c_double, _f64p,
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, _f64p,
+                                             ctypes.POINTER(ctypes.c_int),
+                                             ctypes.POINTER(ctypes.c_int)]
         lib.oracle_nvar_padded.restype = ctypes.c_long
         lib.oracle_nvar_padded.argtypes = [ctypes.c_int]
         _oracle = lib
@@ -135,6 +143,22 @@ def oracle_evaluate(msa: np.ndarray, weights: np.ndarray, lambda_single: float,
                                          float(lambda_single), float(lambda_pair),
                                          _ptr(x64, _f64p), _ptr(g, _f64p))
     return float(f), g
+
+
+def oracle_conjugrad(msa, weights, lambda_single, lambda_pair, x0, max_iter=250, k=5,
+                     max_ls=5, alpha_mul=0.5, ftol=1e-4, wolfe=0.2, eps=0.01):
+    """FP64 host CG with the rules of the device CG: (x, f_hist, iterations, evals, status)."""
+    msa = np.ascontiguousarray(msa, dtype=np.uint8)
+    N, L = msa.shape
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+    fh = np.zeros(max_iter + 1)
+    it, ev = ctypes.c_int(0), ctypes.c_int(0)
+    st = oracle_lib().oracle_conjugrad_f64(_ptr(msa, _u8p), _ptr(w, _f64p), L, N,
+                                           lambda_single, lambda_pair, _ptr(x, _f64p), max_iter,
+                                           k, max_ls, alpha_mul, ftol, wolfe, eps,
+                                           _ptr(fh, _f64p), ctypes.byref(it), ctypes.byref(ev))
+    return x, fh[: it.value + 1], it.value, ev.value, st
 
 
 def oracle_weights(msa: np.ndarray, threshold: float) -> np.ndarray:

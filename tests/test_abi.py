@@ -14,6 +14,7 @@ HEADER = os.path.join(ROOT, "include", "ccmpred_b200.h")
 def declared_functions():
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"^\s*typedef[^;]*;", "", text, flags=re.M | re.S)
     names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_ ]*?[\s\*]+([a-z_][a-z0-9_]*)\s*\(",
                        text, flags=re.M)
     return sorted(set(n for n in names if not n.startswith("sizeof")))

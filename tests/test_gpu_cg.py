@@ -1,0 +1,75 @@
+"""Device conjugate gradient (ccm_conjugrad_gpu) vs an FP64 host CG with the
+same rules (oracle_conjugrad_f64).  libconjugrad is absent from the reference,
+so trajectory parity with the reference optimizer is not pinned; these tests
+check the device loop against its own specification."""
+import numpy as np
+import pytest
+
+from ccmpred_b200 import Evaluator, _lib, synth
+from ccmpred_b200.host import init_bias
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("path", ["tc_bf16x2", "simt_f32"])
+def test_cg_matches_fp64_host_cg(gpu, oracle_mod, path):
+    import torch
+    msa = synth.generate(synth.MSAConfig("cg", 24, 300, n_pairs=4, dup_frac=0.2, seed=61))
+    N, L = msa.shape
+    w = oracle_mod.oracle_weights(msa, 0.8)
+    lam1, lam2 = 0.01, 0.2 * (L - 1)
+    x0 = init_bias(msa)
+    iters = 12
+    xh, fh, it_h, ev_h, st_h = oracle_mod.oracle_conjugrad(msa, w, lam1, lam2, x0,
+                                                          max_iter=iters, eps=0.0)
+    ev = Evaluator(msa, weights=w, lambda_single=lam1, lambda_pair=lam2, path=path)
+    xd = torch.from_numpy(x0.copy()).cuda()
+    seen = []
+    res = ev.minimize(xd, max_iterations=iters, epsilon=0.0,
+                      progress=lambda k, ls, fx, xn, gn, st: seen.append((k, ls, fx)) and False)
+    ev.close()
+    assert res.status == _lib.CG_ERR_MAXITER and st_h == -1023
+    assert res.iterations == it_h == iters
+    assert [k for k, _, _ in seen] == list(range(1, iters + 1))
+    fd = np.array([fx for _, _, fx in seen])
+    assert np.all(np.diff(fd) < 0)                      # monotone decrease
+    assert np.allclose(fd, fh[1:], rtol=2e-5)            # same trajectory as FP64
+    assert abs(res.fx - fh[-1]) / abs(fh[-1]) < 2e-5
+    xg = xd.cpu().numpy().astype(np.float64)
+    assert np.linalg.norm(xg - xh) / np.linalg.norm(xh) < 1e-3
+
+
+def test_cg_converges_and_recovers_planted_contacts(gpu):
+    import torch
+    from ccmpred_b200.host import contact_map
+    cfg = synth.MSAConfig("cg2", 40, 2000, n_pairs=8, seed=62)
+    msa = synth.generate(cfg)
+    N, L = msa.shape
+    from ccmpred_b200 import calculate_weights
+    w = calculate_weights(msa, 0.8)
+    ev = Evaluator(msa, weights=w)
+    xd = torch.from_numpy(init_bias(msa)).cuda()
+    res = ev.minimize(xd, max_iterations=200)
+    ev.close()
+    assert res.status == _lib.CG_SUCCESS and res.iterations < 200
+    cmap, _ = contact_map(xd.cpu().numpy(), L, apc=True)
+    # the planted pairs are the strongest contacts
+    rng = np.random.Generator(np.random.PCG64(cfg.seed))
+    iu = np.triu_indices(L, 1)
+    order = np.argsort(-cmap[iu])
+    top = {(int(iu[0][i]), int(iu[1][i])) for i in order[:8]}
+    planted = planted_pairs(cfg)
+    assert len(top & planted) >= 6, (top, planted)
+
+
+def planted_pairs(cfg):
+    """Re-derive the planted column pairs of synth.generate (same RNG stream)."""
+    from ccmpred_b200.synth import Q
+    rng = np.random.Generator(np.random.PCG64(cfg.seed))
+    L, N = cfg.ncol, cfg.nrow
+    rng.dirichlet(np.full(Q - 1, 0.5), size=L)
+    rng.random((N, L))
+    rng.random((N, L))
+    npairs = min(cfg.n_pairs, L // 2)
+    cols = rng.permutation(L)[: 2 * npairs].reshape(npairs, 2)
+    return {(int(min(a, b)), int(max(a, b))) for a, b in cols}
