@@ -7,14 +7,18 @@
 //
 //   s0 = -g0, alpha0 = 1 / ||g0||
 //   per iteration k:
-//     line search, at most max_linesearch trials x_t = x + alpha s:
-//       accept when f_t <= f + ftol * alpha * (g.s)            (sufficient decrease)
-//                and g_t.s >= wolfe * (g.s)                    (curvature, weak Wolfe)
-//       otherwise alpha *= alpha_mul
+//     line search, at most max_linesearch trials x_t = x + alpha s; accept on
+//       sufficient decrease f_t <= f + ftol * alpha * (g.s); otherwise the
+//       next trial is the minimiser of the quadratic through f, g.s and f_t,
+//       safeguarded to [0.1, alpha_mul] times alpha (N&W sec. 3.5);
+//       if all trials fail and s is not -g, restart along s = -g with
+//       alpha = 1/||g|| and search once more
 //     beta = max(0, g_t.(g_t - g) / g.g)                        (Polak-Ribiere+)
 //     s = -g_t + beta s; if s is not a descent direction, s = -g_t
-//     next alpha = alpha * (g.s_old) / (g_t.s_new)              (N&W eq. 3.60)
+//     next alpha = 2 (f_old - f_new) / -(g_t.s_new)             (N&W eq. 3.60)
 //     stop when k >= K and (f_{k-K} - f_k) / |f_k| < epsilon    ("-e/-k", src/ccmpred.c:192-196)
+//   The reference's "wolfe" parameter (src/ccmpred.c:533) has no role in these
+//   rules; it is kept in ccm_cg_params for the reference's parameter list.
 //
 // Vectors stay in float on the device; every dot product and the line-search
 // tests are FP64.  One trial step (x_t = x + alpha s, the four evaluation
@@ -296,36 +300,56 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
   cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[0], st.d_beta, st.s, n);
   double gs = -gg;  // g.s with s = -g
   double alpha = 1.0 / std::sqrt(gg);
+  bool steepest = true;  // s == -g
   int status = CCM_CG_ERR_MAXITER;
   for (int k = 1; k <= params->max_iterations; ++k) {
     bool accepted = false;
-    int ls = 0;
-    for (ls = 1; ls <= params->max_linesearch; ++ls) {
-      if (!st.trial[p]) {
-        rc = capture_trial(st, p);
-        if (rc != CCM_OK) { free_state(st); return rc; }
+    int ls = 0, trials = 0;
+    for (int attempt = 0; attempt < 2 && !accepted; ++attempt) {
+      for (ls = 1; ls <= params->max_linesearch; ++ls) {
+        if (!st.trial[p]) {
+          rc = capture_trial(st, p);
+          if (rc != CCM_OK) { free_state(st); return rc; }
+        }
+        *st.h_alpha = alpha;
+        e = cudaGraphLaunch(st.trial[p], s);
+        c->launches += st.eval_kernels + 5;  // step + 2 x (dots + final) + evaluation
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+          free_state(st);
+          return set_last_error(CCM_ERR_CUDA, "ccm_conjugrad_gpu: %s", cudaGetErrorString(e));
+        }
+        res.evaluations++;
+        trials++;
+        if (st.h_out->status != 0) {
+          free_state(st);
+          return set_last_error(CCM_ERR_DEVICE, "ccm_conjugrad_gpu: device wait timed out in evaluation");
+        }
+        const double ft = st.h_out->f;
+        if (std::isfinite(ft) && ft <= f + params->ftol * alpha * gs) {
+          accepted = true;
+          break;
+        }
+        const double den = 2.0 * (ft - f - gs * alpha);
+        double aq = (std::isfinite(ft) && den > 0.0) ? -gs * alpha * alpha / den
+                                                    : params->alpha_mul * alpha;
+        aq = std::fmin(aq, params->alpha_mul * alpha);
+        alpha = std::fmax(aq, 0.1 * alpha);
       }
-      *st.h_alpha = alpha;
-      e = cudaGraphLaunch(st.trial[p], s);
-      c->launches += st.eval_kernels + 5;  // step + 2 x (dots + final) + evaluation
-      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-      if (e != cudaSuccess) {
-        free_state(st);
-        return set_last_error(CCM_ERR_CUDA, "ccm_conjugrad_gpu: %s", cudaGetErrorString(e));
-      }
-      res.evaluations++;
-      if (st.h_out->status != 0) {
-        free_state(st);
-        return set_last_error(CCM_ERR_DEVICE, "ccm_conjugrad_gpu: device wait timed out in evaluation");
-      }
-      const double ft = st.h_out->f, gts = st.h_out->gs;
-      if (std::isfinite(ft) && ft <= f + params->ftol * alpha * gs && gts >= params->wolfe * gs) {
-        accepted = true;
+      if (!accepted && !steepest) {
+        // restart along the steepest-descent direction
+        cudaMemsetAsync(st.d_beta, 0, sizeof(double), s);
+        cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[p], st.d_beta, st.s, n);
+        c->launches += 1;
+        gs = -gg;
+        alpha = 1.0 / std::sqrt(gg);
+        steepest = true;
+      } else if (!accepted) {
         break;
       }
-      alpha *= params->alpha_mul;
     }
     if (!accepted) { status = CCM_CG_ERR_LINESEARCH; break; }
+    ls = trials;
     // accept: x, g <- trial buffers
     const double fnew = st.h_out->f, ggnew = st.h_out->gg, gtg = st.h_out->ggold;
     const double xx = st.h_out->xx;
@@ -334,7 +358,7 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
     // Polak-Ribiere+ direction
     double beta = (ggnew - gtg) / gg;
     if (!(beta > 0.0)) beta = 0.0;
-    const double gs_old = gs;
+    steepest = beta == 0.0;
     *st.h_alpha = beta;
     cudaMemcpyAsync(st.d_beta, st.h_alpha, sizeof(double), cudaMemcpyHostToDevice, s);
     cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[p], st.d_beta, st.s, n);
@@ -346,8 +370,9 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
       cudaMemsetAsync(st.d_beta, 0, sizeof(double), s);
       cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[p], st.d_beta, st.s, n);
       gs_new = -ggnew;
+      steepest = true;
     }
-    alpha = alpha * gs_old / gs_new;
+    alpha = 2.0 * (f - fnew) / -gs_new;
     gs = gs_new;
     f = fnew;
     gg = ggnew;

@@ -187,9 +187,10 @@ void oracle_calculate_weights(const unsigned char *msa, int L, int N, float thre
  * ccmpred_b200/csrc/ccm_cg.cu (the optimizer itself is this project's; the
  * reference's libconjugrad is absent, so this is the checker of the device
  * loop, not of libconjugrad).  Same rules: s0 = -g0, alpha0 = 1/||g0||;
- * backtracking line search with sufficient decrease (ftol) and weak Wolfe
- * curvature (wolfe); Polak-Ribiere+ beta with steepest-descent restart;
- * next alpha = alpha * (g.s_old)/(g_new.s_new); stop when
+ * line search on sufficient decrease (ftol) with safeguarded quadratic
+ * backtracking in [0.1, alpha_mul] * alpha, one steepest-descent restart when
+ * max_ls trials fail; Polak-Ribiere+ beta with restart when s is not a
+ * descent direction; next alpha = 2 (f_old - f_new) / -(g.s_new); stop when
  * (f_{i-k} - f_i)/|f_i| < eps.  f_hist receives f after every iteration
  * (f_hist[0] = f(x0)); returns the status code (0 success, -1023 max
  * iterations, -1022 line search failed).
@@ -204,13 +205,14 @@ int oracle_conjugrad_f64(const unsigned char *msa, const double *w, int L, int N
 	double lambda_single, double lambda_pair, double *x, int max_iter, int kwin,
 	int max_ls, double alpha_mul, double ftol, double wolfe, double eps,
 	double *f_hist, int *iterations, int *evaluations) {
+	(void)wolfe;
 	const long n = oracle_nvar_padded(L);
 	double *g = (double *)malloc(sizeof(double) * n);
 	double *gt = (double *)malloc(sizeof(double) * n);
 	double *xt = (double *)malloc(sizeof(double) * n);
 	double *s = (double *)malloc(sizeof(double) * n);
 	double f = oracle_evaluate_f64(msa, w, L, N, lambda_single, lambda_pair, x, g);
-	int evals = 1, status = -1023, it = 0;
+	int evals = 1, status = -1023, it = 0, steepest = 1;
 	f_hist[0] = f;
 	double gg = dot(g, g, n);
 	for (long i = 0; i < n; i++) s[i] = -g[i];
@@ -219,26 +221,39 @@ int oracle_conjugrad_f64(const unsigned char *msa, const double *w, int L, int N
 	for (int k = 1; k <= max_iter; k++) {
 		int ok = 0;
 		double ft = 0.0;
-		for (int ls = 1; ls <= max_ls; ls++) {
-			for (long i = 0; i < n; i++) xt[i] = x[i] + alpha * s[i];
-			ft = oracle_evaluate_f64(msa, w, L, N, lambda_single, lambda_pair, xt, gt);
-			evals++;
-			double gts = dot(gt, s, n);
-			if (isfinite(ft) && ft <= f + ftol * alpha * gs && gts >= wolfe * gs) { ok = 1; break; }
-			alpha *= alpha_mul;
+		for (int attempt = 0; attempt < 2 && !ok; attempt++) {
+			for (int ls = 1; ls <= max_ls; ls++) {
+				for (long i = 0; i < n; i++) xt[i] = x[i] + alpha * s[i];
+				ft = oracle_evaluate_f64(msa, w, L, N, lambda_single, lambda_pair, xt, gt);
+				evals++;
+				if (isfinite(ft) && ft <= f + ftol * alpha * gs) { ok = 1; break; }
+				double den = 2.0 * (ft - f - gs * alpha);
+				double aq = (isfinite(ft) && den > 0.0) ? -gs * alpha * alpha / den : alpha_mul * alpha;
+				aq = fmin(aq, alpha_mul * alpha);
+				alpha = fmax(aq, 0.1 * alpha);
+			}
+			if (!ok && !steepest) {
+				for (long i = 0; i < n; i++) s[i] = -g[i];
+				gs = -gg;
+				alpha = 1.0 / sqrt(gg);
+				steepest = 1;
+			} else if (!ok) {
+				break;
+			}
 		}
 		if (!ok) { status = -1022; break; }
 		double ggnew = dot(gt, gt, n), gtg = dot(gt, g, n), gts_old = dot(gt, s, n);
 		double beta = (ggnew - gtg) / gg;
 		if (!(beta > 0.0)) beta = 0.0;
-		double gs_old = gs;
+		steepest = beta == 0.0;
 		for (long i = 0; i < n; i++) { x[i] = xt[i]; s[i] = beta * s[i] - gt[i]; g[i] = gt[i]; }
 		double gs_new = -ggnew + beta * gts_old;
 		if (!(gs_new < 0.0)) {
 			for (long i = 0; i < n; i++) s[i] = -g[i];
 			gs_new = -ggnew;
+			steepest = 1;
 		}
-		alpha = alpha * gs_old / gs_new;
+		alpha = 2.0 * (f - ft) / -gs_new;
 		gs = gs_new;
 		f = ft;
 		gg = ggnew;
