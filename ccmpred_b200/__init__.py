@@ -59,12 +59,15 @@ def calculate_weights(msa: np.ndarray, threshold: float = 0.8, device: int = 0) 
 class Evaluator:
     """A ccm_context: the alignment, its weights and the device scratch of one path.
 
-    ``path`` is one of ``tc_bf16x2`` (default), ``tc_bf16x3``, ``simt_f32``, ``simt_f64``.
+    ``path`` is one of ``tc_bf16x2`` (default), ``tc_bf16x3``, ``simt_f32``, ``simt_f64``;
+    ``gradient`` is ``tied`` (the reference's g, default) or ``partial`` (true
+    partial derivatives, as autograd needs them).
     """
 
     def __init__(self, msa: np.ndarray, weights: Optional[np.ndarray] = None,
                  lambda_single: float = 0.01, lambda_pair: Optional[float] = None,
-                 path: str = "tc_bf16x2", device: int = 0, stream: Optional[int] = None):
+                 path: str = "tc_bf16x2", device: int = 0, stream: Optional[int] = None,
+                 gradient: str = "tied"):
         self._ctx = ctypes.c_void_p(None)
         self.msa = np.ascontiguousarray(msa, dtype=np.uint8)
         self.N, self.L = self.msa.shape
@@ -80,6 +83,8 @@ class Evaluator:
         opt.path = PATHS[path]
         opt.device = device
         opt.stream = stream
+        opt.gradient = _lib.GRADIENTS[gradient]
+        self.gradient = gradient
         wptr = None
         if weights is not None:
             self.weights = np.ascontiguousarray(weights, dtype=np.float32)

@@ -27,9 +27,15 @@ PATHS = {"tc_bf16x2": PATH_TC_BF16X2, "tc_bf16x3": PATH_TC_BF16X3,
          "simt_f32": PATH_SIMT_F32, "simt_f64": PATH_SIMT_F64}
 
 
+GRADIENT_TIED = 0
+GRADIENT_PARTIAL = 1
+GRADIENTS = {"tied": GRADIENT_TIED, "partial": GRADIENT_PARTIAL}
+
+
 class CcmOptions(ctypes.Structure):
     _fields_ = [("lambda_single", ctypes.c_float), ("lambda_pair", ctypes.c_float),
-                ("path", ctypes.c_int), ("device", ctypes.c_int), ("stream", ctypes.c_void_p)]
+                ("path", ctypes.c_int), ("device", ctypes.c_int), ("stream", ctypes.c_void_p),
+                ("gradient", ctypes.c_int), ("pad", ctypes.c_int)]
 
 
 class CcmResult(ctypes.Structure):

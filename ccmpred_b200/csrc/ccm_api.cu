@@ -154,7 +154,8 @@ int alloc_tc(ccm_context *c) {
   std::vector<int2> tiles;
   const int p_blocks = c->S / 128;
   for (int Q = 0; Q < c->T; ++Q)
-    for (int P = 0; P < p_blocks && P <= 2 * Q + 1; ++P) tiles.push_back(make_int2(P, Q));
+    for (int P = 0; P < p_blocks; ++P)
+      if (c->gradient == CCM_GRADIENT_PARTIAL || P <= 2 * Q + 1) tiles.push_back(make_int2(P, Q));
   c->n_bwd_tiles = (int)tiles.size();
   CCM_CUDA_TRY(cudaMalloc(&c->d_bwd_tiles, sizeof(int2) * tiles.size()));
   CCM_CUDA_TRY(cudaMemcpy(c->d_bwd_tiles, tiles.data(), sizeof(int2) * tiles.size(),
@@ -307,6 +308,7 @@ void ccm_options_default(ccm_options *opt, int ncol) {
   opt->path = CCM_PATH_TC_BF16X2;
   opt->device = 0;
   opt->stream = nullptr;
+  opt->gradient = CCM_GRADIENT_TIED;
 }
 
 int ccm_create(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
@@ -318,6 +320,8 @@ int ccm_create(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
   if (opt) o = *opt; else ccm_options_default(&o, ncol);
   if (o.path < CCM_PATH_TC_BF16X2 || o.path > CCM_PATH_SIMT_F64)
     return set_error(CCM_ERR_INVALID, "ccm_create: unknown path %d", o.path);
+  if (o.gradient != CCM_GRADIENT_TIED && o.gradient != CCM_GRADIENT_PARTIAL)
+    return set_error(CCM_ERR_INVALID, "ccm_create: unknown gradient mode %d", o.gradient);
   for (long long i = 0; i < (long long)ncol * nrow; ++i)
     if (msa[i] > 20) return set_error(CCM_ERR_INVALID, "ccm_create: MSA state %d > 20 at %lld", msa[i], i);
   // the coupling block has 21*32*L^2 entries; keep every index in 32-bit range of int callers
@@ -338,6 +342,7 @@ int ccm_create(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
   c->num_sms = prop.multiProcessorCount;
   c->path = o.path;
   c->nsplit = (o.path == CCM_PATH_TC_BF16X3) ? 3 : 2;
+  c->gradient = o.gradient;
   c->L = ncol;
   c->N = nrow;
   c->nsingle = nsingle_of(ncol);
@@ -348,7 +353,9 @@ int ccm_create(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
   if (o.stream) {
     c->stream = static_cast<cudaStream_t>(o.stream);
   } else {
-    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    // a blocking stream: ordered with the legacy default stream, on which callers
+    // (and torch by default) produce x and consume g
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault);
     if (e != cudaSuccess) { delete c; return set_error(CCM_ERR_CUDA, "stream: %s", cudaGetErrorString(e)); }
     c->own_stream = true;
   }

@@ -29,6 +29,7 @@ struct PrepArgs {
   double *part_reg;
   int L, S;
   float lambda_pair;
+  float g2_coef;  // g2 starts at g2_coef * lambda_pair * x
 };
 
 struct FwdArgs {
@@ -97,6 +98,7 @@ struct ccm_context {
   bool own_stream = false;
   int path = CCM_PATH_TC_BF16X2;
   int nsplit = 2;
+  int gradient = CCM_GRADIENT_TIED;
 
   int L = 0, N = 0;
   long long nsingle = 0, nsp = 0, nvarp = 0;

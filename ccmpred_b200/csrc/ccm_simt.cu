@@ -121,16 +121,18 @@ __global__ void simt_single_kernel(const T *__restrict__ R, T *__restrict__ g1d,
   g1d[v] = s;
 }
 
+// tied (reference): g2 = G2 + G2^T, self blocks 0, + 2 lambda2 x;
+// partial: g2 = G2 (self blocks kept) + lambda2 x -- the true partial derivatives.
 template <typename T>
 __global__ void __launch_bounds__(256) simt_sym_kernel(const T *__restrict__ G2,
                                                        const T *__restrict__ x2,
                                                        T *__restrict__ g2,
                                                        double *__restrict__ part_reg, int L,
-                                                       T lambda_pair) {
+                                                       T lambda_pair, int partial) {
   const int row = blockIdx.x;  // b*L + k
   const int b = row / L, k = row % L;
   const long long QL = (long long)kQ * L;
-  const T two_l2 = (T)2 * lambda_pair;
+  const T two_l2 = (partial ? (T)1 : (T)2) * lambda_pair;
   double acc = 0.0;
   for (int a = 0; a < kQPad; ++a) {
     for (int j = threadIdx.x; j < L; j += blockDim.x) {
@@ -138,7 +140,9 @@ __global__ void __launch_bounds__(256) simt_sym_kernel(const T *__restrict__ G2,
       const T xv = x2[id];
       acc += (double)xv * (double)xv;
       T gv = (T)0;
-      if (a < kQ && k != j)
+      if (a < kQ && partial)
+        gv = G2[(long long)row * QL + (long long)a * L + j];
+      else if (a < kQ && k != j)
         gv = G2[(long long)row * QL + (long long)a * L + j] +
              G2[((long long)a * L + j) * QL + row];
       g2[id] = gv + two_l2 * xv;
@@ -226,7 +230,8 @@ static cudaError_t simt_run(ccm_context *c, const T *d_x, T *d_g) {
   simt_single_kernel<T><<<(nsingle + 127) / 128, 128, 0, c->stream>>>(R, g1d, L, N);
   prof_mark(c);
 
-  simt_sym_kernel<T><<<kQ * L, 256, 0, c->stream>>>(G2, x2, g2, part_reg, L, (T)c->lambda_pair);
+  simt_sym_kernel<T><<<kQ * L, 256, 0, c->stream>>>(G2, x2, g2, part_reg, L, (T)c->lambda_pair,
+                                                     c->gradient == CCM_GRADIENT_PARTIAL);
   prof_mark(c);
 
   simt_finalize_kernel<T><<<1, 1024, 0, c->stream>>>(part_f, N, part_reg, kQ * L, x1, g1d, g1,

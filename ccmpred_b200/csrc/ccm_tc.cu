@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(256) tc_prep_kernel(const float *__restrict__ 
   const int row = blockIdx.x;  // b*L + k
   const int b = row / L, k = row % L;
   const long long base = (long long)row * kQPad * L;
-  const float two_l2 = 2.0f * args.lambda_pair;
+  const float two_l2 = args.g2_coef * args.lambda_pair;  // 2 (tied) or 1 (partial)
   const int nreal = kQ * L;
   double acc = 0.0;
   // rows start at a multiple of 32 L floats (16-byte aligned); L % 4 == 0 allows float4
@@ -470,7 +470,11 @@ struct BwdSmem {
   static constexpr int kTotal = kTOff + kTBytes + 1024;
 };
 
-template <int NSPLIT>
+// SYM = true: C = [O;R]^T [R;O] on the upper triangle of tiles, written to
+// g2 directly and transposed (the reference's tied gradient).  SYM = false:
+// G = O^T R on all tiles, written directly only, self blocks included (the
+// true partial derivatives, for gradient checks and autograd).
+template <int NSPLIT, bool SYM>
 __global__ void __launch_bounds__(kThreads, 1)
     tc_backward_kernel(const __grid_constant__ BwdMaps maps, BwdArgs args) {
   using SM = BwdSmem<NSPLIT>;
@@ -521,15 +525,18 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           uint8_t *st = smem + stage * SM::kStage;
           const int y = kb * kBwdBK;
-          mbar_arrive_expect_tx(&full[stage], SM::kStage);
+          mbar_arrive_expect_tx(&full[stage],
+                                SYM ? SM::kStage : SM::kA + NSPLIT * SM::kB);
           for (int c = 0; c < 2; ++c)
             tma_load_2d(st + SM::kOffOP + c * SM::kChunk, &maps.o, &full[stage], xP + 64 * c, y);
-          for (int i = 0; i < NSPLIT; ++i)
-            for (int c = 0; c < 2; ++c)
-              tma_load_2d(st + SM::kOffRP + i * SM::kA + c * SM::kChunk, &maps.r[i], &full[stage],
-                          xP + 64 * c, y);
-          for (int c = 0; c < 4; ++c)
-            tma_load_2d(st + SM::kOffOQ + c * SM::kChunk, &maps.o, &full[stage], xQ + 64 * c, y);
+          if (SYM) {
+            for (int i = 0; i < NSPLIT; ++i)
+              for (int c = 0; c < 2; ++c)
+                tma_load_2d(st + SM::kOffRP + i * SM::kA + c * SM::kChunk, &maps.r[i],
+                            &full[stage], xP + 64 * c, y);
+            for (int c = 0; c < 4; ++c)
+              tma_load_2d(st + SM::kOffOQ + c * SM::kChunk, &maps.o, &full[stage], xQ + 64 * c, y);
+          }
           for (int i = 0; i < NSPLIT; ++i)
             for (int c = 0; c < 4; ++c)
               tma_load_2d(st + SM::kOffRQ + i * SM::kB + c * SM::kChunk, &maps.r[i], &full[stage],
@@ -579,10 +586,13 @@ __global__ void __launch_bounds__(kThreads, 1)
               const uint64_t dRQ = sdesc_sw128(s0 + SM::kOffRQ + i * SM::kB + ko, SM::kChunk, 1024);
               umma_bf16(d, dOP, dRQ, idesc, (kb | k16 | i) != 0);
             }
+            if (SYM) {
 #pragma unroll
-            for (int i = 0; i < NSPLIT; ++i) {
-              const uint64_t dRP = sdesc_sw128(s0 + SM::kOffRP + i * SM::kA + ko, SM::kChunk, 1024);
-              umma_bf16(d, dRP, dOQ, idesc, 1);
+              for (int i = 0; i < NSPLIT; ++i) {
+                const uint64_t dRP =
+                    sdesc_sw128(s0 + SM::kOffRP + i * SM::kA + ko, SM::kChunk, 1024);
+                umma_bf16(d, dRP, dOQ, idesc, 1);
+              }
             }
           }
           umma_commit(&empty[stage]);
@@ -638,7 +648,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         tmem_wait_ld();
         // (A) transposed writes and the ones-slot column, thread-major
 #pragma unroll
-        for (int i = 0; i < 32; ++i) {
+        for (int i = 0; i < (SYM ? 32 : 0); ++i) {
           const int r2 = c * 32 + i;
           const int s2 = sQ + r2;
           const int a = r2 / kGroupCols, j = jQ + r2 % kGroupCols;
@@ -668,12 +678,12 @@ __global__ void __launch_bounds__(kThreads, 1)
           for (int it = 0; it < 16; ++it) {
             const int row = 2 * it + (lane >> 4);
             const int s1r = rowbase + row;
-            if (s1r > s2) continue;
+            if (SYM && s1r > s2) continue;
             const float val = Tb[row * 17 + col];
             const int tr = s1r / kGroupSlots, rr = s1r % kGroupSlots;
             const int br = rr / kGroupCols, kr = tr * kGroupCols + rr % kGroupCols;
             if (rr < kGroupUsed && kr < L) {
-              if (valid2 && kr != j) atomicAdd(g2 + x2_index(br, kr, a, j, L), val);
+              if (valid2 && (!SYM || kr != j)) atomicAdd(g2 + x2_index(br, kr, a, j, L), val);
             } else if (s1r == kOnesSlot && valid2 && a < kQ - 1) {
               args.g1d[a * L + j] = val;
             }
@@ -746,6 +756,7 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
 
   PrepArgs pa{};
   pa.L = L; pa.S = c->S; pa.lambda_pair = c->lambda_pair; pa.part_reg = c->d_part_reg;
+  pa.g2_coef = c->gradient == CCM_GRADIENT_PARTIAL ? 1.0f : 2.0f;
   for (int i = 0; i < 3; ++i) pa.wperm[i] = c->d_wperm[i];
   prof_mark(c);
   tc_prep_kernel<NSPLIT><<<kQ * L, 256, sizeof(float) * kQ * L, c->stream>>>(x2, g2, pa);
@@ -766,8 +777,12 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
   ba.n_tiles = c->n_bwd_tiles; ba.status = c->d_status; ba.L = L; ba.S = c->S; ba.Npad = c->Npad;
   ba.lambda_pair = c->lambda_pair;
   const int bwd_grid = c->n_bwd_tiles < c->num_sms ? c->n_bwd_tiles : c->num_sms;
-  tc_backward_kernel<NSPLIT><<<bwd_grid, kThreads, BwdSmem<NSPLIT>::kTotal, c->stream>>>(
-      c->bwd_maps, ba);
+  if (c->gradient == CCM_GRADIENT_PARTIAL)
+    tc_backward_kernel<NSPLIT, false><<<bwd_grid, kThreads, BwdSmem<NSPLIT>::kTotal, c->stream>>>(
+        c->bwd_maps, ba);
+  else
+    tc_backward_kernel<NSPLIT, true><<<bwd_grid, kThreads, BwdSmem<NSPLIT>::kTotal, c->stream>>>(
+        c->bwd_maps, ba);
   prof_mark(c);
 
   FinalizeArgs za{};
@@ -794,11 +809,17 @@ cudaError_t tc_configure_kernels() {
   e = cudaFuncSetAttribute(tc_forward_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            FwdSmem<3>::kTotal);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(tc_backward_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           BwdSmem<2>::kTotal);
+  e = cudaFuncSetAttribute(tc_backward_kernel<2, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, BwdSmem<2>::kTotal);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(tc_backward_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              BwdSmem<3>::kTotal);
+  e = cudaFuncSetAttribute(tc_backward_kernel<2, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, BwdSmem<2>::kTotal);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(tc_backward_kernel<3, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, BwdSmem<3>::kTotal);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(tc_backward_kernel<3, false>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, BwdSmem<3>::kTotal);
 }
 
 cudaError_t tc_evaluate(ccm_context *c, const float *d_x, float *d_g) {

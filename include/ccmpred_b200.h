@@ -60,6 +60,13 @@ extern "C" {
 #define CCM_PATH_SIMT_F32 2  /* plain FP32 CUDA-core path (no tensor cores) */
 #define CCM_PATH_SIMT_F64 3  /* FP64 CUDA-core path (gradient checks) */
 
+/* gradient conventions */
+#define CCM_GRADIENT_TIED 0    /* the reference's g: coupling part along the tied direction
+                                  W(b,k,a,j) = W(a,j,b,k), self-edge blocks zeroed, 2 lambda2 W
+                                  (src/evaluate_cpu.c:131-163) */
+#define CCM_GRADIENT_PARTIAL 1 /* true partial derivatives of f w.r.t. every entry of x: untied
+                                  G2 + lambda2 W, self blocks included (gradient checks, autograd) */
+
 typedef struct ccm_context ccm_context;
 
 typedef struct ccm_options {
@@ -67,7 +74,10 @@ typedef struct ccm_options {
 	float lambda_pair;   /* default 0.2 * (L - 1) (src/ccmpred.c:224,502-503) */
 	int path;            /* CCM_PATH_* ; default CCM_PATH_TC_BF16X2 */
 	int device;          /* CUDA device ordinal; default 0 */
-	void *stream;        /* cudaStream_t to run on, or NULL for a private stream */
+	void *stream;        /* cudaStream_t to run on, or NULL for a private stream that is
+	                        ordered with the legacy default stream */
+	int gradient;        /* CCM_GRADIENT_*; default CCM_GRADIENT_TIED */
+	int pad;
 } ccm_options;
 
 /* Result of the last evaluation, as kept on the device. */
