@@ -121,8 +121,6 @@ constexpr int kFwdBM = 128, kFwdBN = 256, kFwdBK = 32;
 // forward: warp 0 TMA, warp 1 MMA, warps 2-9 epilogue (two warps per TMEM lane
 // quarter, each owning half of the 256 accumulator columns)
 constexpr int kFwdThreads = 320;
-// backward: warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
-constexpr int kThreads = 192;
 
 template <int NSPLIT>
 struct FwdSmem {
@@ -451,6 +449,15 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
 
 // -------------------------------------------------------------- tc_backward
 constexpr int kBwdBM = 128, kBwdBN = 256, kBwdBK = 32;
+// The K loop (rows of the alignment) is cut into chunks of kBwdChunkKB k-blocks
+// (512 rows).  Each chunk is accumulated by the tensor cores into one of the two
+// TMEM buffers, and the epilogue adds the finished chunk into FP32 registers
+// (round-to-nearest).  The tensor-core accumulator then never sums more than
+// one chunk, which keeps its rounding error from growing with N.
+constexpr int kBwdChunkKB = 16;
+// warp 0 TMA, warp 1 MMA, warps 2-9 epilogue (two warps per TMEM lane quarter,
+// one per half of the 256 columns)
+constexpr int kBwdThreads = 320;
 
 template <int NSPLIT>
 struct BwdSmem {
@@ -466,7 +473,7 @@ struct BwdSmem {
   static constexpr int kStage = kOffRQ + NSPLIT * kB;
   static constexpr int kBarOff = kStages * kStage;
   static constexpr int kTOff = kBarOff + 256;                    // epilogue transpose buffers
-  static constexpr int kTBytes = 4 * 32 * 17 * 4;                // 4 warps x 32 rows x 16(+1) cols
+  static constexpr int kTBytes = 8 * 32 * 9 * 4;                 // 8 warps x 32 rows x 8(+1) cols
   static constexpr int kTotal = kTOff + kTBytes + 1024;
 };
 
@@ -475,7 +482,7 @@ struct BwdSmem {
 // G = O^T R on all tiles, written directly only, self blocks included (the
 // true partial derivatives, for gradient checks and autograd).
 template <int NSPLIT, bool SYM>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kBwdThreads, 1)
     tc_backward_kernel(const __grid_constant__ BwdMaps maps, BwdArgs args) {
   using SM = BwdSmem<NSPLIT>;
   constexpr int kStages = SM::kStages;
@@ -495,7 +502,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
-    for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 4); }
+    for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 8); }
     mbar_init(drain, 1);
     *abort_flag = 0;
     fence_mbar_init();
@@ -554,75 +561,110 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (lane == 0) {
       constexpr uint32_t idesc = idesc_bf16_f32(kBwdBM, kBwdBN, 1, 1);
       uint32_t it = 0;
-      int local = 0;
-      for (int tile = blockIdx.x; tile < n_tiles && !aborted(abort_flag);
-           tile += gridDim.x, ++local) {
-        const int acc = local & 1;
-        const uint32_t use = local >> 1;
-        if (!mbar_wait(&tempty[acc], (use & 1) ^ 1)) {
-          record_error(args.status, kErrBwdTimeout, abort_flag);
-          break;
-        }
-        tc_fence_after();
-        const uint32_t d = tmem_base + acc * kBwdBN;
-        bool ok = true;
-        for (int kb = 0; kb < k_blocks; ++kb, ++it) {
-          const int stage = it % kStages;
-          const uint32_t round = it / kStages;
-          if (!mbar_wait(&full[stage], round & 1)) {
+      uint32_t chunk = 0;  // chunks issued by this CTA, across tiles
+      bool ok = true;
+      for (int tile = blockIdx.x; tile < n_tiles && ok && !aborted(abort_flag);
+           tile += gridDim.x) {
+        for (int kb0 = 0; kb0 < k_blocks && ok; kb0 += kBwdChunkKB, ++chunk) {
+          const int buf = chunk & 1;
+          const uint32_t use = chunk >> 1;
+          if (!mbar_wait(&tempty[buf], (use & 1) ^ 1)) {
             record_error(args.status, kErrBwdTimeout, abort_flag);
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t s0 = smem_u32(smem + stage * SM::kStage);
-#pragma unroll
-          for (int k16 = 0; k16 < kBwdBK / 16; ++k16) {
-            const uint32_t ko = k16 * 16 * 128;
-            const uint64_t dOP = sdesc_sw128(s0 + SM::kOffOP + ko, SM::kChunk, 1024);
-            const uint64_t dOQ = sdesc_sw128(s0 + SM::kOffOQ + ko, SM::kChunk, 1024);
-#pragma unroll
-            for (int i = 0; i < NSPLIT; ++i) {
-              const uint64_t dRQ = sdesc_sw128(s0 + SM::kOffRQ + i * SM::kB + ko, SM::kChunk, 1024);
-              umma_bf16(d, dOP, dRQ, idesc, (kb | k16 | i) != 0);
+          const uint32_t d = tmem_base + buf * kBwdBN;
+          const int kb1 = min(kb0 + kBwdChunkKB, k_blocks);
+          for (int kb = kb0; kb < kb1; ++kb, ++it) {
+            const int stage = it % kStages;
+            const uint32_t round = it / kStages;
+            if (!mbar_wait(&full[stage], round & 1)) {
+              record_error(args.status, kErrBwdTimeout, abort_flag);
+              ok = false;
+              break;
             }
-            if (SYM) {
+            tc_fence_after();
+            const uint32_t s0 = smem_u32(smem + stage * SM::kStage);
+#pragma unroll
+            for (int k16 = 0; k16 < kBwdBK / 16; ++k16) {
+              const uint32_t ko = k16 * 16 * 128;
+              const uint64_t dOP = sdesc_sw128(s0 + SM::kOffOP + ko, SM::kChunk, 1024);
+              const uint64_t dOQ = sdesc_sw128(s0 + SM::kOffOQ + ko, SM::kChunk, 1024);
 #pragma unroll
               for (int i = 0; i < NSPLIT; ++i) {
-                const uint64_t dRP =
-                    sdesc_sw128(s0 + SM::kOffRP + i * SM::kA + ko, SM::kChunk, 1024);
-                umma_bf16(d, dRP, dOQ, idesc, 1);
+                const uint64_t dRQ =
+                    sdesc_sw128(s0 + SM::kOffRQ + i * SM::kB + ko, SM::kChunk, 1024);
+                umma_bf16(d, dOP, dRQ, idesc, ((kb - kb0) | k16 | i) != 0);
+              }
+              if (SYM) {
+#pragma unroll
+                for (int i = 0; i < NSPLIT; ++i) {
+                  const uint64_t dRP =
+                      sdesc_sw128(s0 + SM::kOffRP + i * SM::kA + ko, SM::kChunk, 1024);
+                  umma_bf16(d, dRP, dOQ, idesc, 1);
+                }
               }
             }
+            umma_commit(&empty[stage]);
           }
-          umma_commit(&empty[stage]);
+          if (!ok) break;
+          umma_commit(&tfull[buf]);
         }
-        if (!ok) break;
-        umma_commit(&tfull[acc]);
       }
       umma_commit(drain);
       if (!mbar_wait(drain, 0)) record_error(args.status, kErrBwdTimeout, abort_flag);
     }
   } else {
-    // Epilogue.  Element (s1, s2), s1 <= s2, of the symmetric C goes to
+    // Epilogue.  Each thread owns one row s1 of the tile (TMEM lane) and one
+    // half of its 256 columns; it sums the tile's K chunks in FP32 registers,
+    // then writes every element (s1, s2), s1 <= s2, of the symmetric C to
     //   direct      g2 row (b,k) = s1, column (a,j) = s2
     //   transposed  g2 row (a,j) = s2, column (b,k) = s1   (s1 != s2)
-    // Transposed writes are issued thread-major (consecutive lanes = consecutive
-    // k: contiguous runs).  Direct writes go through a per-warp shared-memory
-    // transpose so that one warp instruction covers 2 rows x 16 columns, i.e.
-    // runs of consecutive j, instead of 32 different rows.
-    // g2 already holds 2*lambda2*x (tc_prep); every element receives exactly
-    // one atomic add of its C value (none on self-edge blocks), so the result
-    // does not depend on the order of the adds.
+    // (SYM = false: direct only, all elements).  Transposed writes are issued
+    // thread-major (consecutive lanes = consecutive k: contiguous runs); direct
+    // writes go through a per-warp shared-memory transpose so that one warp
+    // instruction covers 4 rows x 8 columns (runs of consecutive j).  g2 already
+    // holds the regulariser term (tc_prep) and every element receives exactly one
+    // atomic add, so the result does not depend on the order of the adds.
     const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
     const int L = args.L;
     float *__restrict__ g2 = args.g2;
-    float *Tb = reinterpret_cast<float *>(smem + SM::kTOff) + (warp - 2) * 32 * 17;
-    int local = 0;
-    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++local) {
-      if (__shfl_sync(0xffffffffu, aborted(abort_flag) ? 1 : 0, 0)) break;
-      const int acc = local & 1;
-      const uint32_t use = local >> 1;
+    float *Tb = reinterpret_cast<float *>(smem + SM::kTOff) + (warp - 2) * 32 * 9;
+    uint32_t chunk = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+      float accv[128];
+#pragma unroll
+      for (int i = 0; i < 128; ++i) accv[i] = 0.0f;
+      for (int kb0 = 0; kb0 < k_blocks; kb0 += kBwdChunkKB, ++chunk) {
+        const int buf = chunk & 1;
+        const uint32_t use = chunk >> 1;
+        const bool w_ok = mbar_wait(&tfull[buf], use & 1);
+        if (__any_sync(0xffffffffu, !w_ok)) {
+          if (lane == 0) record_error(args.status, kErrBwdTimeout, abort_flag);
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t taddr =
+            tmem_base + buf * kBwdBN + half * 128 + ((uint32_t)(q * 32) << 16);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          uint32_t v[32];
+          __syncwarp();
+          tmem_ld32(taddr + c * 32, v);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 32; ++i) accv[c * 32 + i] += __uint_as_float(v[i]);
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tempty[buf]);
+      }
+      if (!ok) break;
+
       const int2 pq = args.tiles[tile];
       const int rowbase = pq.x * kBwdBM + q * 32;
       const int s1 = rowbase + lane;
@@ -630,69 +672,53 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int b = r1 / kGroupCols, k = t1 * kGroupCols + r1 % kGroupCols;
       const bool valid1 = r1 < kGroupUsed && k < L;
       const long long colt = (long long)b * L + k;  // transposed: + ((a*L+j)*32)*L
-      const int sQ = pq.y * kBwdBN;
-      const int jQ = pq.y * kGroupCols;
-
-      bool ok = mbar_wait(&tfull[acc], use & 1);
-      if (__any_sync(0xffffffffu, !ok)) {
-        if (lane == 0) record_error(args.status, kErrBwdTimeout, abort_flag);
-        break;
-      }
-      tc_fence_after();
-      const uint32_t taddr = tmem_base + acc * kBwdBN + ((uint32_t)(q * 32) << 16);
-#pragma unroll 1
-      for (int c = 0; c < 8; ++c) {
-        uint32_t v[32];
+      const int sQ = pq.y * kBwdBN + half * 128;
+      // 16 rounds of 8 columns through the transpose buffer Tb[row][col]
+#pragma unroll
+      for (int cb = 0; cb < 16; ++cb) {
         __syncwarp();
-        tmem_ld32(taddr + c * 32, v);
-        tmem_wait_ld();
-        // (A) transposed writes and the ones-slot column, thread-major
 #pragma unroll
-        for (int i = 0; i < (SYM ? 32 : 0); ++i) {
-          const int r2 = c * 32 + i;
-          const int s2 = sQ + r2;
-          const int a = r2 / kGroupCols, j = jQ + r2 % kGroupCols;
-          const bool valid2 = r2 < kGroupUsed && j < L;
-          const float cval = __uint_as_float(v[i]);
-          if (s1 < s2) {
-            if (valid1 && valid2) {
-              if (k != j) atomicAdd(g2 + ((long long)a * L + j) * kQPad * L + colt, cval);
-            } else if (s2 == kOnesSlot && valid1 && b < kQ - 1) {
-              args.g1d[b * L + k] = cval;
+        for (int e = 0; e < 8; ++e) Tb[lane * 9 + e] = accv[cb * 8 + e];
+        __syncwarp();
+        // (A) transposed writes and the ones-slot column: thread = row s1
+        if (SYM) {
+#pragma unroll 1
+          for (int col = 0; col < 8; ++col) {
+            const int r2 = half * 128 + cb * 8 + col;
+            const int s2 = sQ + cb * 8 + col;
+            const int a = r2 / kGroupCols, j = pq.y * kGroupCols + r2 % kGroupCols;
+            const bool valid2 = r2 < kGroupUsed && j < L;
+            if (s1 < s2) {
+              const float val = Tb[lane * 9 + col];
+              if (valid1 && valid2) {
+                if (k != j) atomicAdd(g2 + ((long long)a * L + j) * kQPad * L + colt, val);
+              } else if (s2 == kOnesSlot && valid1 && b < kQ - 1) {
+                args.g1d[b * L + k] = val;
+              }
             }
           }
         }
-        // (B) direct writes and the ones-slot row, through the transpose buffer
+        // (B) direct writes and the ones-slot row: lanes = 4 rows x 8 columns
+        const int col = lane & 7;
+        const int r2 = half * 128 + cb * 8 + col;
+        const int s2 = sQ + cb * 8 + col;
+        const int a = r2 / kGroupCols, j = pq.y * kGroupCols + r2 % kGroupCols;
+        const bool valid2 = r2 < kGroupUsed && j < L;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          __syncwarp();
-#pragma unroll
-          for (int e = 0; e < 16; ++e) Tb[lane * 17 + e] = __uint_as_float(v[h * 16 + e]);
-          __syncwarp();
-          const int col = lane & 15;
-          const int r2 = c * 32 + h * 16 + col;
-          const int s2 = sQ + r2;
-          const int a = r2 / kGroupCols, j = jQ + r2 % kGroupCols;
-          const bool valid2 = r2 < kGroupUsed && j < L;
-#pragma unroll 4
-          for (int it = 0; it < 16; ++it) {
-            const int row = 2 * it + (lane >> 4);
-            const int s1r = rowbase + row;
-            if (SYM && s1r > s2) continue;
-            const float val = Tb[row * 17 + col];
-            const int tr = s1r / kGroupSlots, rr = s1r % kGroupSlots;
-            const int br = rr / kGroupCols, kr = tr * kGroupCols + rr % kGroupCols;
-            if (rr < kGroupUsed && kr < L) {
-              if (valid2 && (!SYM || kr != j)) atomicAdd(g2 + x2_index(br, kr, a, j, L), val);
-            } else if (s1r == kOnesSlot && valid2 && a < kQ - 1) {
-              args.g1d[a * L + j] = val;
-            }
+        for (int it = 0; it < 8; ++it) {
+          const int row = 4 * it + (lane >> 3);
+          const int s1r = rowbase + row;
+          if (SYM && s1r > s2) continue;
+          const float val = Tb[row * 9 + col];
+          const int tr = s1r / kGroupSlots, rr = s1r % kGroupSlots;
+          const int br = rr / kGroupCols, kr = tr * kGroupCols + rr % kGroupCols;
+          if (rr < kGroupUsed && kr < L) {
+            if (valid2 && (!SYM || kr != j)) atomicAdd(g2 + x2_index(br, kr, a, j, L), val);
+          } else if (s1r == kOnesSlot && valid2 && a < kQ - 1) {
+            args.g1d[a * L + j] = val;
           }
         }
       }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&tempty[acc]);
     }
   }
 
@@ -778,10 +804,10 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
   ba.lambda_pair = c->lambda_pair;
   const int bwd_grid = c->n_bwd_tiles < c->num_sms ? c->n_bwd_tiles : c->num_sms;
   if (c->gradient == CCM_GRADIENT_PARTIAL)
-    tc_backward_kernel<NSPLIT, false><<<bwd_grid, kThreads, BwdSmem<NSPLIT>::kTotal, c->stream>>>(
+    tc_backward_kernel<NSPLIT, false><<<bwd_grid, kBwdThreads, BwdSmem<NSPLIT>::kTotal, c->stream>>>(
         c->bwd_maps, ba);
   else
-    tc_backward_kernel<NSPLIT, true><<<bwd_grid, kThreads, BwdSmem<NSPLIT>::kTotal, c->stream>>>(
+    tc_backward_kernel<NSPLIT, true><<<bwd_grid, kBwdThreads, BwdSmem<NSPLIT>::kTotal, c->stream>>>(
         c->bwd_maps, ba);
   prof_mark(c);
 
