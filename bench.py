@@ -56,6 +56,12 @@ def parse_args():
     p.add_argument("--cpu-budget-s", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-precision", action="store_true")
+    p.add_argument("--workload", default="L300_N5000", choices=["L300_N5000", "batch256"],
+                   help="batch256: 256 ragged alignments solved to convergence (MSAs/s)")
+    p.add_argument("--batch-workers", type=int, default=8)
+    p.add_argument("--batch-plain-sample", type=int, default=8)
+    p.add_argument("--ref-cuda-steps", type=int, default=3,
+                   help="evaluations of the reference's own CUDA kernels (sm_100a build); 0 = skip")
     return p.parse_args()
 
 
@@ -234,6 +240,34 @@ def precision_block(msa, w, x, g_gpu, f_gpu, L):
             "reference": "FP64 oracle (oracle/ccm_oracle.c) at the same x and weights"}
 
 
+def reference_cuda_timing(msa, x, xd, steps, with_precision):
+    """The reference's own CUDA evaluator (evaluate_cuda.c + evaluate_cuda_kernels.cu built
+    for sm_100a from its sources), same x, device pointers, host-synchronised like the
+    reference (it returns f by value and syncs after every kernel)."""
+    import torch
+    from oracle import oracle as O
+    if not os.path.exists(O.REF_CUDA_SO):
+        return {"unavailable": "oracle/_ref/libccmref_cuda.so was not built"}
+    N, L = msa.shape
+    ev = O.RefCudaEvaluator(msa, 0.01, 0.2 * (L - 1), 0.8)
+    g = torch.empty_like(xd)
+    f = ev.evaluate(xd.data_ptr(), g.data_ptr())
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ev.evaluate(xd.data_ptr(), g.data_ptr())
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    out = {"evals_per_s": steps / el, "steps": steps,
+           "impl": "reference evaluate_cuda + evaluate_cuda_kernels.cu compiled for sm_100a "
+                   "(SIMT FP32, fdexp/fdlog = expf/logf)"}
+    if with_precision:
+        w = O.ref_calculate_weights(msa, 0.8)
+        out["precision"] = precision_block(msa, w, x, g.cpu().numpy(), f, L)
+    ev.close()
+    return out
+
+
 def traffic_from_profiles(kernel: str):
     path = os.path.join(ROOT, "profiles", "tc_kernels_L300_N5000.json")
     if not os.path.exists(path):
@@ -244,9 +278,62 @@ def traffic_from_profiles(kernel: str):
     return None if k is None else k.get("dram_bytes_per_launch")
 
 
+def run_batch(args, world, rank, local):
+    """256 ragged alignments (L ~ U[50,400], N ~ logU[200,20000]) solved to convergence
+    (eps 1e-3 or 250 iterations) concurrently, vs one at a time on the plain FP32 path
+    (timed on a stratified sample and extrapolated)."""
+    import torch
+    import ccmpred_b200 as cb
+    from ccmpred_b200 import synth
+    torch.cuda.set_device(local)
+    msas = synth.batch_workload(256, seed0=1000 + 1000 * rank)
+    cb.solve_batch(msas[:2], workers=2, max_iterations=3, epsilon=1e-3, device=local)  # warm-up
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    res, _ = cb.solve_batch(msas, workers=args.batch_workers, max_iterations=250, epsilon=1e-3,
+                            device=local)
+    torch.cuda.synchronize()
+    el = max_over_ranks(world, time.perf_counter() - t0)
+    value = world * len(msas) / el
+    if rank != 0:
+        return
+    cost = np.array([m.shape[0] * m.shape[1] ** 2 for m in msas], dtype=np.float64)
+    order = np.argsort(cost)
+    k = args.batch_plain_sample
+    sample = [int(order[int((i + 0.5) * len(order) / k)]) for i in range(k)]
+    plain_t = []
+    for i in sample:
+        t1 = time.perf_counter()
+        cb.solve_batch([msas[i]], workers=1, path="simt_f32", max_iterations=250, epsilon=1e-3,
+                       device=local)
+        plain_t.append(time.perf_counter() - t1)
+    plain_total = float(np.sum(plain_t) * len(msas) / k)
+    its = np.array([r.iterations for r in res])
+    ok = sum(r.status in (0, -1023) for r in res)
+    print(json.dumps({
+        "metric": "MSAs/s, 256 ragged alignments solved to convergence", "value": value,
+        "unit": "MSAs/s", "n_gpus": world, "higher_is_better": True, "scaling": "weak",
+        "data": "synthetic", "dtype": "bf16",
+        "config": {"workload": "batch256: L~U[50,400], N~logU[200,20000], seeds 1000+i, "
+                               "eps 1e-3 or 250 iterations",
+                   "workers": args.batch_workers, "path": "tc_bf16x2"},
+        "wall_s": el, "solved_ok": ok, "iterations_mean": float(its.mean()),
+        "plain_f32_one_at_a_time": {
+            "msas_per_s_extrapolated": len(msas) / plain_total,
+            "sample": f"{k} alignments stratified by N*L^2, timed one at a time, "
+                      f"scaled to {len(msas)}",
+            "speedup": value / (len(msas) / plain_total)},
+    }))
+
+
 def main():
     args = parse_args()
     world, rank, local = dist_init(args)
+    if args.impl == "b200" and args.workload == "batch256":
+        run_batch(args, world, rank, local)
+        barrier(world)
+        return
     if args.impl == "reference":
         run_reference_arm(args, world, rank)
         barrier(world)
@@ -357,6 +444,10 @@ def main():
             prec = {args.path: precision_block(msa, w, x, g_gpu, f_gpu, L)}
             if plain is not None:
                 prec["simt_f32"] = precision_block(msa, w, x, g_plain, f_plain, L)
+        ref_cuda = None
+        if args.ref_cuda_steps > 0 and world == 1:
+            ref_cuda = reference_cuda_timing(msa, x, xd, args.ref_cuda_steps,
+                                             not args.no_precision)
         cpu = None
         if not args.no_cpu_baseline and world == 1:
             v, n_ev, kind, cores = cpu_reference_timing(msa, x, args.cpu_budget_s, 10)
@@ -385,6 +476,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks,
             "plain_f32": plain,
+            "reference_cuda": ref_cuda,
             "precision": prec,
             "init_ms": {"weights": init_ms},
         }

@@ -56,6 +56,33 @@ def calculate_weights(msa: np.ndarray, threshold: float = 0.8, device: int = 0) 
     return w
 
 
+def solve_batch(msas, workers: int = 8, path: str = "tc_bf16x2", threshold: float = 0.8,
+                max_iterations: int = 250, epsilon: float = 0.01, contact_maps: bool = True,
+                device: int = 0):
+    """Solve many alignments to convergence concurrently (ccm_solve_batch).
+
+    Returns (results, maps): per-alignment CcmBatchResult and APC contact maps."""
+    arrs = [np.ascontiguousarray(m, dtype=np.uint8) for m in msas]
+    n = len(arrs)
+    descs = (_lib.CcmMsaDesc * max(n, 1))()
+    for i, a in enumerate(arrs):
+        descs[i].msa = a.ctypes.data
+        descs[i].nrow, descs[i].ncol = a.shape
+    p = _lib.CcmBatchParams()
+    lib().ccm_batch_params_default(ctypes.byref(p))
+    p.workers, p.path, p.reweighting_threshold, p.device = workers, PATHS[path], threshold, device
+    p.cg.max_iterations, p.cg.epsilon = max_iterations, epsilon
+    res = (_lib.CcmBatchResult * max(n, 1))()
+    maps = [np.empty((a.shape[1], a.shape[1]), dtype=np.float32) for a in arrs] if contact_maps else None
+    mptr = None
+    if maps is not None:
+        mptr = (ctypes.POINTER(ctypes.c_float) * max(n, 1))()
+        for i, m in enumerate(maps):
+            mptr[i] = m.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    check(lib().ccm_solve_batch(n, descs, ctypes.byref(p), res, mptr))
+    return [res[i] for i in range(n)], maps
+
+
 class Evaluator:
     """A ccm_context: the alignment, its weights and the device scratch of one path.
 

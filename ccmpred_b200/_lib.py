@@ -72,6 +72,23 @@ CG_ERR_MAXITER = -1023
 CG_ERR_LINESEARCH = -1022
 CG_ERR_NONFINITE = -1021
 
+class CcmMsaDesc(ctypes.Structure):
+    _fields_ = [("msa", ctypes.c_void_p), ("ncol", ctypes.c_int), ("nrow", ctypes.c_int)]
+
+
+class CcmBatchParams(ctypes.Structure):
+    _fields_ = [("reweighting_threshold", ctypes.c_float), ("lambda_single", ctypes.c_float),
+                ("lambda_pair_factor", ctypes.c_float), ("path", ctypes.c_int),
+                ("workers", ctypes.c_int), ("device", ctypes.c_int), ("use_apc", ctypes.c_int),
+                ("pad", ctypes.c_int), ("cg", CcmCgParams)]
+
+
+class CcmBatchResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("iterations", ctypes.c_int),
+                ("evaluations", ctypes.c_int), ("pad", ctypes.c_int),
+                ("fx", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+
 # progress(instance, x, g, fx, xnorm, gnorm, step, n, k, ls) -> int
 PROGRESS = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                             ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
@@ -113,6 +130,11 @@ SIGNATURES = {
                                          PROGRESS, _vp, ctypes.POINTER(CcmCgResult)]),
     "ccm_conjugrad_host": (ctypes.c_int, [_vp, _f32p, ctypes.c_longlong, ctypes.POINTER(CcmCgParams),
                                           PROGRESS, _vp, ctypes.POINTER(CcmCgResult)]),
+    "ccm_batch_params_default": (None, [ctypes.POINTER(CcmBatchParams)]),
+    "ccm_solve_batch": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(CcmMsaDesc),
+                                       ctypes.POINTER(CcmBatchParams),
+                                       ctypes.POINTER(CcmBatchResult),
+                                       ctypes.POINTER(ctypes.POINTER(ctypes.c_float))]),
     "ccm_device_count": (ctypes.c_int, []),
     "ccm_device_info": (ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_size_t),

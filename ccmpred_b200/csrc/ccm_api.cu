@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include <cuda.h>
@@ -70,16 +71,18 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+EncodeTiledFn lookup_encode_fn() {
+  void *p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+          cudaSuccess &&
+      q == cudaDriverEntryPointSuccess)
+    return reinterpret_cast<EncodeTiledFn>(p);
+  return nullptr;
+}
+
 EncodeTiledFn get_encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void *p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiledFn>(p);
-  }
+  static const EncodeTiledFn fn = lookup_encode_fn();  // thread-safe one-time init
   return fn;
 }
 
@@ -124,9 +127,11 @@ __global__ void build_onehot_kernel(const uint8_t *__restrict__ msa, __nv_bfloat
 }
 
 bool configured[64] = {false};
+std::mutex configure_mutex;
 
 int ensure_configured(int device) {
   if (device < 0 || device >= 64) return set_error(CCM_ERR_INVALID, "bad device %d", device);
+  std::lock_guard<std::mutex> lock(configure_mutex);
   if (configured[device]) return CCM_OK;
   CCM_CUDA_TRY(tc_configure_kernels());
   CCM_CUDA_TRY(simt_configure_kernels());

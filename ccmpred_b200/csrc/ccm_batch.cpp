@@ -1,0 +1,105 @@
+// Many alignments solved to convergence concurrently: a pool of host worker
+// threads, each driving its own context (and CUDA stream) through the
+// reweighting, init_bias, the device conjugate gradient and the APC contact
+// map.  Alignments are handed out largest-first (cost ~ N L^2) so that the
+// long solves start early.  Small alignments leave most of the GPU idle on
+// their own; running several at once on separate streams fills it.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ccmpred_b200.h"
+
+extern "C" {
+
+void ccm_batch_params_default(ccm_batch_params *p) {
+  if (!p) return;
+  p->reweighting_threshold = 0.8f;
+  p->lambda_single = 0.01f;
+  p->lambda_pair_factor = 0.2f;
+  p->path = CCM_PATH_TC_BF16X2;
+  p->workers = 8;
+  p->device = 0;
+  p->use_apc = 1;
+  p->pad = 0;
+  ccm_cg_params_default(&p->cg);
+}
+
+int ccm_solve_batch(int n, const ccm_msa_desc *msas, const ccm_batch_params *params,
+                    ccm_batch_result *results, float **contact_maps) {
+  if (n < 0 || (n > 0 && (!msas || !results)) || !params || params->workers < 1) return CCM_ERR_INVALID;
+  for (int i = 0; i < n; ++i)
+    if (!msas[i].msa || msas[i].ncol <= 0 || msas[i].nrow <= 0) return CCM_ERR_INVALID;
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::sort(order.begin(), order.end(), [&](int a, int b) {
+    const double ca = (double)msas[a].nrow * msas[a].ncol * msas[a].ncol;
+    const double cb = (double)msas[b].nrow * msas[b].ncol * msas[b].ncol;
+    return ca > cb;
+  });
+  std::atomic<int> next(0);
+  std::atomic<int> first_error(CCM_OK);
+
+  auto work = [&]() {
+    cudaSetDevice(params->device);
+    for (;;) {
+      const int slot = next.fetch_add(1);
+      if (slot >= n || first_error.load() != CCM_OK) break;
+      const int i = order[slot];
+      const ccm_msa_desc &m = msas[i];
+      ccm_batch_result &r = results[i];
+      std::memset(&r, 0, sizeof(r));
+      const auto t0 = std::chrono::steady_clock::now();
+      const int L = m.ncol, N = m.nrow;
+      std::vector<float> w(N, 1.0f);
+      int rc = CCM_OK;
+      if (params->reweighting_threshold < 1.0f)
+        rc = ccm_calculate_weights(m.msa, L, N, params->reweighting_threshold, w.data(),
+                                   params->device);
+      const long long nv = ccm_nvar_padded(L);
+      std::vector<float> x(rc == CCM_OK ? (size_t)nv : 0);
+      ccm_context *ctx = nullptr;
+      if (rc == CCM_OK) {
+        ccm_init_bias(m.msa, L, N, x.data());
+        ccm_options o;
+        ccm_options_default(&o, L);
+        o.lambda_single = params->lambda_single;
+        o.lambda_pair = params->lambda_pair_factor * (float)(L - 1);
+        o.path = params->path;
+        o.device = params->device;
+        rc = ccm_create(&ctx, m.msa, L, N, w.data(), &o);
+      }
+      ccm_cg_result cg;
+      std::memset(&cg, 0, sizeof(cg));
+      if (rc == CCM_OK) rc = ccm_conjugrad_host(ctx, x.data(), nv, &params->cg, nullptr, nullptr, &cg);
+      if (ctx) ccm_destroy(ctx);
+      if (rc == CCM_OK && contact_maps && contact_maps[i]) {
+        ccm_sum_submatrices(x.data(), contact_maps[i], L);
+        if (params->use_apc) ccm_apc(contact_maps[i], L);
+      }
+      r.status = rc == CCM_OK ? cg.status : rc;
+      r.iterations = cg.iterations;
+      r.evaluations = cg.evaluations;
+      r.fx = cg.fx;
+      r.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      if (rc != CCM_OK) {
+        int expected = CCM_OK;
+        first_error.compare_exchange_strong(expected, rc);
+      }
+    }
+  };
+  const int nw = std::min(params->workers, std::max(n, 1));
+  std::vector<std::thread> threads;
+  for (int t = 0; t < nw; ++t) threads.emplace_back(work);
+  for (auto &t : threads) t.join();
+  return first_error.load();
+}
+
+}  // extern "C"

@@ -110,3 +110,15 @@ def _symmetrise(W: np.ndarray) -> np.ndarray:
     M = W.reshape(n, n)
     U = np.triu(M, 1)
     return (U + U.T + np.diag(np.diag(M))).reshape(W.shape).astype(np.float32)
+
+
+def batch_workload(n: int = 256, seed0: int = 1000):
+    """Ragged batch: n alignments, L ~ U[50, 400], N ~ logU[200, 20000], alignment i
+    generated from seed seed0 + i (10 % gaps, L // 10 planted pairs)."""
+    out = []
+    for i in range(n):
+        rng = np.random.Generator(np.random.PCG64(seed0 + i))
+        L = int(rng.integers(50, 401))
+        N = int(round(np.exp(rng.uniform(np.log(200), np.log(20000)))))
+        out.append(generate(MSAConfig(f"batch{i}", L, N, n_pairs=L // 10, seed=seed0 + i)))
+    return out

@@ -254,6 +254,45 @@ CCM_API int ccm_conjugrad_host(ccm_context *ctx, float *x, long long n,
                                const ccm_cg_params *params, ccm_progress_t progress,
                                void *instance, ccm_cg_result *result);
 
+/* ---------------------------------------------------------------- batched solves */
+/* Many alignments of different sizes solved to convergence concurrently on
+ * one GPU (no reference counterpart: the reference runs one alignment per
+ * process).  Host worker threads each drive their own context and stream
+ * through reweighting, init_bias, the device CG and the contact map;
+ * alignments are taken largest-first. */
+typedef struct ccm_msa_desc {
+	const unsigned char *msa;   /* nrow x ncol states 0..20, host memory */
+	int ncol;
+	int nrow;
+} ccm_msa_desc;
+
+typedef struct ccm_batch_params {
+	float reweighting_threshold; /* 0.8 */
+	float lambda_single;         /* 0.01 */
+	float lambda_pair_factor;    /* 0.2: lambda_pair = factor * (L - 1) */
+	int path;                    /* CCM_PATH_* */
+	int workers;                 /* concurrent solves (threads / streams), default 8 */
+	int device;
+	int use_apc;                 /* contact maps with APC (1) or raw Frobenius norms (0) */
+	int pad;
+	ccm_cg_params cg;            /* optimizer settings for every alignment */
+} ccm_batch_params;
+
+typedef struct ccm_batch_result {
+	int status;        /* CCM_CG_* of the solve, or a CCM_ERR_* code */
+	int iterations;
+	int evaluations;
+	int pad;
+	double fx;
+	double seconds;    /* wall time of this alignment's solve */
+} ccm_batch_result;
+
+CCM_API void ccm_batch_params_default(ccm_batch_params *p);
+/* results[i] for msas[i]; contact_maps may be NULL or hold n pointers (each
+ * NULL or ncol*ncol floats) that receive the APC-corrected maps. */
+CCM_API int ccm_solve_batch(int n, const ccm_msa_desc *msas, const ccm_batch_params *params,
+                            ccm_batch_result *results, float **contact_maps);
+
 /* Devices (src/ccmpred.c:400-478 device selection and memory report). */
 CCM_API int ccm_device_count(void);
 CCM_API int ccm_device_info(int device, char *name, int name_len, size_t *mem_free,

@@ -274,6 +274,42 @@ def ref_read_raw(path: str, L: int) -> np.ndarray:
     return x
 
 
+class RefCudaEvaluator:
+    """The reference's CUDA backend (src/evaluate_cuda.c + src/evaluate_cuda_kernels.cu,
+    built for sm_100a by oracle/Makefile) behind init_cuda/evaluate_cuda/destroy_cuda.
+    x and g are device pointers.  The reference keeps its device state in process
+    globals: one instance per process at a time."""
+
+    def __init__(self, msa: np.ndarray, lambda_single: float, lambda_pair: float,
+                 threshold: float):
+        lib = ctypes.CDLL(REF_CUDA_SO)
+        vp = ctypes.c_void_p
+        lib.ref_userdata_new.restype = vp
+        lib.ref_userdata_new.argtypes = [_u8p, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_float, ctypes.c_float, ctypes.c_float]
+        lib.ref_userdata_free.argtypes = [vp]
+        lib.init_cuda.argtypes = [vp]
+        lib.destroy_cuda.argtypes = [vp]
+        lib.evaluate_cuda.restype = ctypes.c_float
+        lib.evaluate_cuda.argtypes = [vp, vp, vp, ctypes.c_int]
+        self.lib = lib
+        self.msa = np.ascontiguousarray(msa, dtype=np.uint8)
+        self.N, self.L = self.msa.shape
+        self.ud = lib.ref_userdata_new(_ptr(self.msa, _u8p), self.L, self.N,
+                                       lambda_single, lambda_pair, threshold)
+        lib.init_cuda(self.ud)
+        self.nvar = nvar_padded(self.L)
+
+    def evaluate(self, d_x: int, d_g: int) -> float:
+        return float(self.lib.evaluate_cuda(self.ud, d_x, d_g, self.nvar))
+
+    def close(self):
+        if self.ud:
+            self.lib.destroy_cuda(self.ud)
+            self.lib.ref_userdata_free(self.ud)
+            self.ud = None
+
+
 def time_ref_evaluate(msa: np.ndarray, x: np.ndarray, lambda_single: float, lambda_pair: float,
                       threshold: float, omp: bool, repeats: int = 1,
                       budget_s: Optional[float] = None):
