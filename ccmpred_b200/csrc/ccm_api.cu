@@ -163,8 +163,8 @@ int alloc_tc(ccm_context *c) {
       if (c->gradient == CCM_GRADIENT_PARTIAL || P <= 2 * Q + 1) tiles.push_back(make_int2(P, Q));
   c->n_bwd_tiles = (int)tiles.size();
   CCM_CUDA_TRY(cudaMalloc(&c->d_bwd_tiles, sizeof(int2) * tiles.size()));
-  CCM_CUDA_TRY(cudaMemcpy(c->d_bwd_tiles, tiles.data(), sizeof(int2) * tiles.size(),
-                          cudaMemcpyHostToDevice));
+  CCM_CUDA_TRY(cudaMemcpyAsync(c->d_bwd_tiles, tiles.data(), sizeof(int2) * tiles.size(),
+                               cudaMemcpyHostToDevice, c->stream));
 
   const long long total = (long long)Np * S;
   build_onehot_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c->stream>>>(

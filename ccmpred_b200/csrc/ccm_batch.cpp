@@ -13,9 +13,12 @@
 #include <thread>
 #include <vector>
 
+#include <mutex>
+#include <string>
+
 #include <cuda_runtime.h>
 
-#include "../../include/ccmpred_b200.h"
+#include "ccm_internal.cuh"
 
 extern "C" {
 
@@ -46,9 +49,22 @@ int ccm_solve_batch(int n, const ccm_msa_desc *msas, const ccm_batch_params *par
   });
   std::atomic<int> next(0);
   std::atomic<int> first_error(CCM_OK);
+  std::mutex err_mutex;
+  std::string err_text;
 
   auto work = [&]() {
     cudaSetDevice(params->device);
+    // a non-blocking stream per worker: no implicit ordering with the legacy
+    // default stream, which would interfere with the CG's graph capture while
+    // other workers are running
+    cudaStream_t stream = nullptr;
+    if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) {
+      int expected = CCM_OK;
+      first_error.compare_exchange_strong(expected, CCM_ERR_CUDA);
+      std::lock_guard<std::mutex> lock(err_mutex);
+      err_text = "ccm_solve_batch: cannot create a worker stream";
+      return;
+    }
     for (;;) {
       const int slot = next.fetch_add(1);
       if (slot >= n || first_error.load() != CCM_OK) break;
@@ -74,6 +90,7 @@ int ccm_solve_batch(int n, const ccm_msa_desc *msas, const ccm_batch_params *par
         o.lambda_pair = params->lambda_pair_factor * (float)(L - 1);
         o.path = params->path;
         o.device = params->device;
+        o.stream = stream;
         rc = ccm_create(&ctx, m.msa, L, N, w.data(), &o);
       }
       ccm_cg_result cg;
@@ -91,15 +108,21 @@ int ccm_solve_batch(int n, const ccm_msa_desc *msas, const ccm_batch_params *par
       r.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
       if (rc != CCM_OK) {
         int expected = CCM_OK;
-        first_error.compare_exchange_strong(expected, rc);
+        if (first_error.compare_exchange_strong(expected, rc)) {
+          std::lock_guard<std::mutex> lock(err_mutex);
+          err_text = std::string("alignment ") + std::to_string(i) + ": " + ccm_last_error();
+        }
       }
     }
+    cudaStreamDestroy(stream);
   };
   const int nw = std::min(params->workers, std::max(n, 1));
   std::vector<std::thread> threads;
   for (int t = 0; t < nw; ++t) threads.emplace_back(work);
   for (auto &t : threads) t.join();
-  return first_error.load();
+  const int rc = first_error.load();
+  if (rc != CCM_OK) ccm::set_last_error(rc, "ccm_solve_batch: %s", err_text.c_str());
+  return rc;
 }
 
 }  // extern "C"
