@@ -450,11 +450,11 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
 // -------------------------------------------------------------- tc_backward
 constexpr int kBwdBM = 128, kBwdBN = 256, kBwdBK = 32;
 // The K loop (rows of the alignment) is cut into chunks of kBwdChunkKB k-blocks
-// (512 rows).  Each chunk is accumulated by the tensor cores into one of the two
+// (1024 rows).  Each chunk is accumulated by the tensor cores into one of the two
 // TMEM buffers, and the epilogue adds the finished chunk into FP32 registers
 // (round-to-nearest).  The tensor-core accumulator then never sums more than
 // one chunk, which keeps its rounding error from growing with N.
-constexpr int kBwdChunkKB = 16;
+constexpr int kBwdChunkKB = 32;
 // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue (two warps per TMEM lane quarter,
 // one per half of the 256 columns)
 constexpr int kBwdThreads = 320;
