@@ -133,7 +133,9 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_init(args):
+def dist_init(args=None, backend: str = "nccl"):
+    """One process per GPU (torchrun env).  NCCL carries only the barrier and the
+    max-over-ranks timing: the workload is replicated, nothing is exchanged."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -142,8 +144,9 @@ def dist_init(args):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
@@ -158,7 +161,8 @@ def max_over_ranks(world, value: float) -> float:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
