@@ -142,7 +142,8 @@ int ensure_configured(int device) {
 int alloc_tc(ccm_context *c) {
   c->T = n_groups(c->L);
   c->S = c->T * kGroupSlots;
-  c->Npad = ((c->N + 127) / 128) * 128;
+  // rows padded to the forward's 256-row CTA-pair tiles
+  c->Npad = ((c->N + 255) / 256) * 256;
   const size_t S = c->S, Np = c->Npad;
   CCM_CUDA_TRY(cudaMalloc(&c->d_onehot, sizeof(__nv_bfloat16) * Np * S));
   for (int i = 0; i < c->nsplit; ++i) {
@@ -345,6 +346,13 @@ int ccm_create(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
   ccm_context *c = new ccm_context();
   c->device = o.device;
   c->num_sms = prop.multiProcessorCount;
+  if (o.path == CCM_PATH_TC_BF16X2 || o.path == CCM_PATH_TC_BF16X3) {
+    cudaError_t e = tc_forward_max_pairs(o.path == CCM_PATH_TC_BF16X3 ? 3 : 2, &c->fwd_pairs);
+    if (e != cudaSuccess || c->fwd_pairs < 1) {
+      delete c;
+      return set_error(CCM_ERR_CUDA, "tc_forward cluster occupancy: %s", cudaGetErrorString(e));
+    }
+  }
   c->path = o.path;
   c->nsplit = (o.path == CCM_PATH_TC_BF16X3) ? 3 : 2;
   c->gradient = o.gradient;

@@ -73,6 +73,8 @@ void prof_mark(ccm_context *c);
 void count_launch(ccm_context *c, int n = 1);
 
 cudaError_t tc_configure_kernels();
+// CTA pairs of tc_forward that can be resident at once on the current device.
+cudaError_t tc_forward_max_pairs(int nsplit, int *pairs);
 cudaError_t tc_evaluate(ccm_context *c, const float *d_x, float *d_g);
 int tc_fwd_smem_bytes(int nsplit);
 int tc_bwd_smem_bytes(int nsplit);
@@ -94,6 +96,7 @@ cudaError_t reweight_counts(const uint8_t *d_msa, int L, int N, int idthres, int
 struct ccm_context {
   int device = 0;
   int num_sms = 148;
+  int fwd_pairs = 74;             // resident CTA pairs of tc_forward
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int path = CCM_PATH_TC_BF16X2;

@@ -43,20 +43,30 @@ __global__ void __launch_bounds__(256) tc_prep_kernel(const float *__restrict__ 
   double acc = 0.0;
   // rows start at a multiple of 32 L floats (16-byte aligned); L % 4 == 0 allows float4
   if ((L & 3) == 0) {
+    // the whole 32 L row as float4: four independent 16-byte loads in flight per
+    // thread; the real states (first 21 L floats) are also staged in shared memory
     const float4 *src = reinterpret_cast<const float4 *>(x2 + base);
     float4 *dst = reinterpret_cast<float4 *>(g2 + base);
-    for (int i = threadIdx.x; i < nreal / 4; i += blockDim.x) {
-      const float4 v = src[i];
-      acc += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w;
-      reinterpret_cast<float4 *>(xrow)[i] = v;
-      dst[i] = make_float4(two_l2 * v.x, two_l2 * v.y, two_l2 * v.z, two_l2 * v.w);
-    }
-    const float4 *srcp = reinterpret_cast<const float4 *>(x2 + base + nreal);
-    float4 *dstp = reinterpret_cast<float4 *>(g2 + base + nreal);
-    for (int i = threadIdx.x; i < (kQPad - kQ) * L / 4; i += blockDim.x) {
-      const float4 v = srcp[i];
-      acc += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w;
-      dstp[i] = make_float4(two_l2 * v.x, two_l2 * v.y, two_l2 * v.z, two_l2 * v.w);
+    const int n4 = kQPad * L / 4, nreal4 = nreal / 4;
+    constexpr int kU = 4;
+    for (int i0 = threadIdx.x; i0 < n4; i0 += kU * blockDim.x) {
+      float4 v[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int i = i0 + u * blockDim.x;
+        v[u] = i < n4 ? __ldcs(src + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int i = i0 + u * blockDim.x;
+        if (i < n4) {
+          acc += (double)v[u].x * v[u].x + (double)v[u].y * v[u].y + (double)v[u].z * v[u].z +
+                 (double)v[u].w * v[u].w;
+          if (i < nreal4) reinterpret_cast<float4 *>(xrow)[i] = v[u];
+          __stcs(dst + i, make_float4(two_l2 * v[u].x, two_l2 * v[u].y, two_l2 * v[u].z,
+                                      two_l2 * v[u].w));
+        }
+      }
     }
   } else {
     for (int i = threadIdx.x; i < nreal; i += blockDim.x) {
@@ -117,16 +127,22 @@ __global__ void __launch_bounds__(256) tc_prep_kernel(const float *__restrict__ 
 }
 
 // --------------------------------------------------------------- tc_forward
+// The forward runs on CTA pairs (clusters of 2): one pair MMA of M = 256 rows x
+// N = 256 slots per K step, each CTA holding 128 of the rows (kFwdBM) and 128 of
+// the slot columns of B.  Per CTA and K step that is half the B bytes of a
+// single-CTA 128 x 256 tile, which is what keeps the tensor pipe fed.
 constexpr int kFwdBM = 128, kFwdBN = 256, kFwdBK = 32;
-// forward: warp 0 TMA, warp 1 MMA, warps 2-9 epilogue (two warps per TMEM lane
-// quarter, each owning half of the 256 accumulator columns)
+constexpr int kFwdPairM = 2 * kFwdBM;   // rows per pair tile
+constexpr int kFwdHalfN = kFwdBN / 2;   // B columns held by each CTA
+// forward: warp 0 TMA, warp 1 MMA (leader CTA), warps 2-9 epilogue (two warps per
+// TMEM lane quarter, each owning half of the 256 accumulator columns)
 constexpr int kFwdThreads = 320;
 
 template <int NSPLIT>
 struct FwdSmem {
-  static constexpr int kStages = NSPLIT == 2 ? 5 : 3;
+  static constexpr int kStages = NSPLIT == 2 ? 8 : 6;
   static constexpr int kABytes = kFwdBM * kFwdBK * 2;            // 8 KB, K-major, 64B swizzle
-  static constexpr int kBBytes = kFwdBN * kFwdBK * 2;            // 16 KB per term, MN-major
+  static constexpr int kBBytes = kFwdHalfN * kFwdBK * 2;         // 8 KB per term, MN-major
   static constexpr int kStage = kABytes + NSPLIT * kBBytes;
   static constexpr int kBarOff = kStages * kStage;
   static constexpr int kVOff = kBarOff + 256;                     // V of the tile's 12 columns
@@ -157,7 +173,7 @@ __device__ __forceinline__ bool aborted(const int *abort_flag) {
 template <int NSPLIT, int H>
 __device__ __forceinline__ void fwd_epilogue_tile(const FwdArgs &args, uint32_t taddr, const float *Vs,
                                                   float *xbuf, int q, int lane, int n, int t,
-                                                  long long tile) {
+                                                  long long part) {
   const int L = args.L;
   const int j0 = t * kGroupCols;
   const bool live = n < args.N;
@@ -277,16 +293,19 @@ __device__ __forceinline__ void fwd_epilogue_tile(const FwdArgs &args, uint32_t 
   }
   // loss partial, one per (tile, epilogue warp), summed in fixed order by tc_finalize
   for (int o = 16; o > 0; o >>= 1) floss += __shfl_xor_sync(0xffffffffu, floss, o);
-  if (lane == 0) args.part_f[tile * 8 + H * 4 + q] = floss;
+  if (lane == 0) args.part_f[part * 8 + H * 4 + q] = floss;
 }
 
 template <int NSPLIT>
-__global__ void __launch_bounds__(kFwdThreads, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kFwdThreads, 1)
     tc_forward_kernel(const __grid_constant__ FwdMaps maps, FwdArgs args) {
   using SM = FwdSmem<NSPLIT>;
   constexpr int kFwdStages = SM::kStages;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = align1024(smem_raw);
+  // barriers: full[] is used in the leader only (it counts the bytes of both
+  // CTAs' loads); empty[] and tfull[] in both (the leader's commits reach both);
+  // tempty[] in the leader only (all 16 epilogue warps of the pair arrive there)
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + SM::kBarOff);
   uint64_t *empty = full + kFwdStages;
   uint64_t *tfull = empty + kFwdStages;
@@ -298,12 +317,14 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
   float *xbuf = reinterpret_cast<float *>(smem + SM::kXOff);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n_tiles = args.m_tiles * args.T;
+  const uint32_t rank = cluster_ctarank();
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+  const int n_tiles = args.m_tiles * args.T;  // m_tiles counts 256-row pair tiles
   const int k_blocks = args.S / kFwdBK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kFwdStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
-    for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 8); }
+    for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 16); }
     mbar_init(drain, 1);
     *abort_flag = 0;
     fence_mbar_init();
@@ -312,18 +333,21 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
     prefetch_tmap(&maps.a);
     for (int i = 0; i < NSPLIT; ++i) prefetch_tmap(&maps.b[i]);
   }
-  if (warp == 1) { tmem_alloc(tmem_slot, 512); tmem_relinquish(); }
+  if (warp == 1) { tmem_alloc_pair(tmem_slot, 512); tmem_relinquish_pair(); }
+  // both CTAs' barriers initialised and TMEM allocated before any remote use
   tc_fence_before();
-  __syncthreads();
+  cluster_sync();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
   if (warp == 0) {
     if (lane == 0) {
-      // ---------------- TMA producer
+      // ---------------- TMA producer (both CTAs): own A rows, own half of B
       uint32_t it = 0;
-      for (int tile = blockIdx.x; tile < n_tiles && !aborted(abort_flag); tile += gridDim.x) {
+      for (int tile = pair; tile < n_tiles && !aborted(abort_flag); tile += npairs) {
         const int m = tile % args.m_tiles, t = tile / args.m_tiles;
+        const int row0 = m * kFwdPairM + (int)rank * kFwdBM;
+        const int col0 = t * kFwdBN + (int)rank * kFwdHalfN;
         for (int kb = 0; kb < k_blocks; ++kb, ++it) {
           const int stage = it % kFwdStages;
           const uint32_t round = it / kFwdStages;
@@ -332,32 +356,37 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
             break;
           }
           uint8_t *sa = smem + stage * SM::kStage;
-          mbar_arrive_expect_tx(&full[stage], SM::kStage);
-          tma_load_2d(sa, &maps.a, &full[stage], kb * kFwdBK, m * kFwdBM);
+          const uint32_t fb = mapa_shared(smem_u32(&full[stage]), 0);
+          if (rank == 0) mbar_arrive_expect_tx(&full[stage], 2 * SM::kStage);
+          tma_load_2d_pair(sa, &maps.a, fb, kb * kFwdBK, row0);
           for (int i = 0; i < NSPLIT; ++i) {
             uint8_t *sb = sa + SM::kABytes + i * SM::kBBytes;
-            for (int c = 0; c < 4; ++c)
-              tma_load_2d(sb + c * (kFwdBK * 128), &maps.b[i], &full[stage],
-                          t * kFwdBN + c * 64, kb * kFwdBK);
+            for (int c = 0; c < kFwdHalfN / 64; ++c)
+              tma_load_2d_pair(sb + c * (kFwdBK * 128), &maps.b[i], fb, col0 + c * 64,
+                               kb * kFwdBK);
           }
         }
       }
-      // drain: every issued load must land before the CTA may exit
+      // drain: every issued load must land before the CTA may exit.  The leader
+      // sees both CTAs' bytes on its full barriers; the other CTA sees the MMA's
+      // release of each stage (issued after the stage's loads were consumed).
       const uint32_t issued = it;
-      for (uint32_t r = (issued > kFwdStages ? issued - kFwdStages : 0); r < issued; ++r)
-        if (!mbar_wait(&full[r % kFwdStages], (r / kFwdStages) & 1)) {
+      for (uint32_t r = (issued > kFwdStages ? issued - kFwdStages : 0); r < issued; ++r) {
+        const bool ok = rank == 0 ? mbar_wait(&full[r % kFwdStages], (r / kFwdStages) & 1)
+                                  : mbar_wait(&empty[r % kFwdStages], (r / kFwdStages) & 1);
+        if (!ok) {
           record_error(args.status, kErrFwdTimeout, abort_flag);
           break;
         }
+      }
     }
   } else if (warp == 1) {
-    if (lane == 0) {
-      // ---------------- MMA issuer
-      constexpr uint32_t idesc = idesc_bf16_f32(kFwdBM, kFwdBN, 0, 1);
+    if (lane == 0 && rank == 0) {
+      // ---------------- MMA issuer (leader CTA): 256 x 256 x 16 pair MMAs
+      constexpr uint32_t idesc = idesc_bf16_f32(kFwdPairM, kFwdBN, 0, 1);
       uint32_t it = 0;
       int local = 0;
-      for (int tile = blockIdx.x; tile < n_tiles && !aborted(abort_flag);
-           tile += gridDim.x, ++local) {
+      for (int tile = pair; tile < n_tiles && !aborted(abort_flag); tile += npairs, ++local) {
         const int acc = local & 1;
         const uint32_t use = local >> 1;
         if (!mbar_wait(&tempty[acc], (use & 1) ^ 1)) {
@@ -385,26 +414,26 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
             for (int i = 0; i < NSPLIT; ++i) {
               const uint64_t bd =
                   sdesc_sw128(b0 + i * SM::kBBytes + k16 * 16 * 128, kFwdBK * 128, 1024);
-              umma_bf16(d, ad, bd, idesc, (kb | k16 | i) != 0);
+              umma_bf16_pair(d, ad, bd, idesc, (kb | k16 | i) != 0);
             }
           }
-          umma_commit(&empty[stage]);
+          umma_commit_pair(&empty[stage], 0x3);
         }
         if (!ok) break;
-        umma_commit(&tfull[acc]);
+        umma_commit_pair(&tfull[acc], 0x3);
       }
-      umma_commit(drain);
+      umma_commit_pair(drain, 0x1);
       if (!mbar_wait(drain, 0)) record_error(args.status, kErrFwdTimeout, abort_flag);
     }
   } else {
-    // ---------------- epilogue: 8 warps; warp w owns TMEM lanes 32*(w%4) ...
-    // and column half (w-2)/4
+    // ---------------- epilogue (both CTAs): 8 warps; warp w owns TMEM lanes
+    // 32*(w%4) ... and column half (w-2)/4 of this CTA's 128 rows
     const int q = warp & 3;
     const int half = (warp - 2) >> 2;
     const int ethr = threadIdx.x - 64;
     const int L = args.L;
     int local = 0;
-    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++local) {
+    for (int tile = pair; tile < n_tiles; tile += npairs, ++local) {
       // all eight epilogue warps agree here: every one finished the previous
       // tile (so Vs may be overwritten) and none has seen an abort
       if (named_bar_or(1, 256, aborted(abort_flag))) break;
@@ -417,7 +446,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
         Vs[ethr] = (j < L) ? args.x1[a * L + j] : 0.0f;
       }
       named_bar_sync(1, 256);
-      const int n = m * kFwdBM + q * 32 + lane;
+      const int n = m * kFwdPairM + (int)rank * kFwdBM + q * 32 + lane;
       bool ok = mbar_wait(&tfull[acc], use & 1);
       if (__any_sync(0xffffffffu, !ok)) {
         // leave through the agreement barrier at the top of the loop; the
@@ -427,23 +456,26 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
       }
       tc_fence_after();
       const uint32_t taddr = tmem_base + acc * kFwdBN + ((uint32_t)(q * 32) << 16);
+      const long long part = (long long)tile * 2 + rank;
       if (half == 0)
-        fwd_epilogue_tile<NSPLIT, 0>(args, taddr, Vs, xbuf, q, lane, n, t, tile);
+        fwd_epilogue_tile<NSPLIT, 0>(args, taddr, Vs, xbuf, q, lane, n, t, part);
       else
-        fwd_epilogue_tile<NSPLIT, 1>(args, taddr, Vs, xbuf, q, lane, n, t, tile);
-      // accumulator may be reused by the MMA warp
+        fwd_epilogue_tile<NSPLIT, 1>(args, taddr, Vs, xbuf, q, lane, n, t, part);
+      // accumulator may be reused by the leader's MMA warp
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(&tempty[acc]);
+      if (lane == 0) mbar_arrive_cluster(mapa_shared(smem_u32(&tempty[acc]), 0));
     }
   }
 
+  // neither CTA leaves while the other may still read its shared memory or
+  // signal its barriers
   tc_fence_before();
-  __syncthreads();
+  cluster_sync();
   if (warp == 1) {
     __syncwarp();
     tc_fence_after();
-    tmem_dealloc(tmem_base, 512);
+    tmem_dealloc_pair(tmem_base, 512);
   }
 }
 
@@ -791,10 +823,12 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
   FwdArgs fa{};
   fa.msa = c->d_msa; fa.w = c->d_w; fa.x1 = x1; fa.part_f = c->d_part_f; fa.status = c->d_status;
   for (int i = 0; i < 3; ++i) fa.r[i] = c->d_r[i];
-  fa.L = L; fa.N = c->N; fa.S = c->S; fa.T = c->T; fa.Npad = c->Npad; fa.m_tiles = c->Npad / kFwdBM;
-  const int fwd_tiles = fa.m_tiles * c->T;
-  const int fwd_grid = fwd_tiles < c->num_sms ? fwd_tiles : c->num_sms;
-  tc_forward_kernel<NSPLIT><<<fwd_grid, kFwdThreads, FwdSmem<NSPLIT>::kTotal, c->stream>>>(
+  fa.L = L; fa.N = c->N; fa.S = c->S; fa.T = c->T; fa.Npad = c->Npad;
+  fa.m_tiles = c->Npad / kFwdPairM;
+  const int pair_tiles = fa.m_tiles * c->T;
+  const int fwd_tiles = 2 * pair_tiles;  // 128-row halves, one loss partial set each
+  const int pairs = pair_tiles < c->fwd_pairs ? pair_tiles : c->fwd_pairs;
+  tc_forward_kernel<NSPLIT><<<2 * pairs, kFwdThreads, FwdSmem<NSPLIT>::kTotal, c->stream>>>(
       c->fwd_maps, fa);
   prof_mark(c);
 
@@ -820,6 +854,19 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
   prof_mark(c);
   count_launch(c, 4);
   return cudaGetLastError();
+}
+
+cudaError_t tc_forward_max_pairs(int nsplit, int *pairs) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2, 1, 1);
+  cfg.blockDim = dim3(kFwdThreads, 1, 1);
+  cfg.dynamicSmemBytes = nsplit == 3 ? FwdSmem<3>::kTotal : FwdSmem<2>::kTotal;
+  int n = 0;
+  cudaError_t e = nsplit == 3
+                      ? cudaOccupancyMaxActiveClusters(&n, tc_forward_kernel<3>, &cfg)
+                      : cudaOccupancyMaxActiveClusters(&n, tc_forward_kernel<2>, &cfg);
+  *pairs = n;
+  return e;
 }
 
 cudaError_t tc_configure_kernels() {

@@ -34,7 +34,7 @@ def expected_internals(msa, w, x, L, lam2):
     N = msa.shape[0]
     T = (L + G - 1) // G
     S = T * 256
-    Npad = (N + 127) // 128 * 128
+    Npad = (N + 255) // 256 * 256  # rows padded to the forward's 256-row pair tiles
     nsp = 20 * L + 32 - (20 * L) % 32
     V = x[:20 * L].reshape(20, L).astype(np.float64)
     W = x[nsp:].reshape(Q, L, QP, L)[:, :, :Q, :].astype(np.float64)      # [b,k,a,j]
