@@ -158,10 +158,11 @@ int alloc_tc(ccm_context *c) {
   CCM_CUDA_TRY(cudaMalloc(&c->d_g1d, sizeof(float) * (kQ - 1) * c->L));
 
   std::vector<int2> tiles;
-  const int p_blocks = c->S / 128;
+  // P and Q in 256-slot blocks (rows, columns of C); the symmetric gradient
+  // needs only the tiles that hold some s1 <= s2
   for (int Q = 0; Q < c->T; ++Q)
-    for (int P = 0; P < p_blocks; ++P)
-      if (c->gradient == CCM_GRADIENT_PARTIAL || P <= 2 * Q + 1) tiles.push_back(make_int2(P, Q));
+    for (int P = 0; P < c->T; ++P)
+      if (c->gradient == CCM_GRADIENT_PARTIAL || P <= Q) tiles.push_back(make_int2(P, Q));
   c->n_bwd_tiles = (int)tiles.size();
   CCM_CUDA_TRY(cudaMalloc(&c->d_bwd_tiles, sizeof(int2) * tiles.size()));
   CCM_CUDA_TRY(cudaMemcpyAsync(c->d_bwd_tiles, tiles.data(), sizeof(int2) * tiles.size(),
@@ -347,8 +348,10 @@ int ccm_create(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
   c->device = o.device;
   c->num_sms = prop.multiProcessorCount;
   if (o.path == CCM_PATH_TC_BF16X2 || o.path == CCM_PATH_TC_BF16X3) {
-    cudaError_t e = tc_forward_max_pairs(o.path == CCM_PATH_TC_BF16X3 ? 3 : 2, &c->fwd_pairs);
-    if (e != cudaSuccess || c->fwd_pairs < 1) {
+    const int ns = o.path == CCM_PATH_TC_BF16X3 ? 3 : 2;
+    cudaError_t e = tc_forward_max_pairs(ns, &c->fwd_pairs);
+    if (e == cudaSuccess) e = tc_backward_max_pairs(ns, &c->bwd_pairs);
+    if (e != cudaSuccess || c->fwd_pairs < 1 || c->bwd_pairs < 1) {
       delete c;
       return set_error(CCM_ERR_CUDA, "tc_forward cluster occupancy: %s", cudaGetErrorString(e));
     }

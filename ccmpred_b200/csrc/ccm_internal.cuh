@@ -75,6 +75,7 @@ void count_launch(ccm_context *c, int n = 1);
 cudaError_t tc_configure_kernels();
 // CTA pairs of tc_forward that can be resident at once on the current device.
 cudaError_t tc_forward_max_pairs(int nsplit, int *pairs);
+cudaError_t tc_backward_max_pairs(int nsplit, int *pairs);
 cudaError_t tc_evaluate(ccm_context *c, const float *d_x, float *d_g);
 int tc_fwd_smem_bytes(int nsplit);
 int tc_bwd_smem_bytes(int nsplit);
@@ -97,6 +98,7 @@ struct ccm_context {
   int device = 0;
   int num_sms = 148;
   int fwd_pairs = 74;             // resident CTA pairs of tc_forward
+  int bwd_pairs = 74;             // resident CTA pairs of tc_backward
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int path = CCM_PATH_TC_BF16X2;

@@ -480,23 +480,30 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kFwdThreads, 1)
 }
 
 // -------------------------------------------------------------- tc_backward
+// Like the forward, the backward runs on CTA pairs: a pair tile is 256 slots P
+// (C rows, 128 per CTA) x kBwdBN slots Q (C columns, half of the B operand per
+// CTA).  N = 256 keeps the operand bytes per MMA clock low enough for shared
+// memory to feed the tensor pipe (N = 128 tiles measured 25 % slower).
 constexpr int kBwdBM = 128, kBwdBN = 256, kBwdBK = 32;
+constexpr int kBwdPairM = 2 * kBwdBM;
+constexpr int kBwdHalfN = kBwdBN / 2;
+constexpr int kBwdBufs = 512 / kBwdBN;  // TMEM accumulators of kBwdBN columns
 // The K loop (rows of the alignment) is cut into chunks of kBwdChunkKB k-blocks
-// (1024 rows).  Each chunk is accumulated by the tensor cores into one of the two
+// (1280 rows).  Each chunk is accumulated by the tensor cores into one of the two
 // TMEM buffers, and the epilogue adds the finished chunk into FP32 registers
 // (round-to-nearest).  The tensor-core accumulator then never sums more than
 // one chunk, which keeps its rounding error from growing with N.
-constexpr int kBwdChunkKB = 32;
-// warp 0 TMA, warp 1 MMA, warps 2-9 epilogue (two warps per TMEM lane quarter,
-// one per half of the 256 columns)
+constexpr int kBwdChunkKB = 40;
+// warp 0 TMA, warp 1 MMA (leader CTA), warps 2-9 epilogue (two warps per TMEM
+// lane quarter, one per half of the 256 columns)
 constexpr int kBwdThreads = 320;
 
 template <int NSPLIT>
 struct BwdSmem {
-  static constexpr int kStages = NSPLIT == 2 ? 3 : 2;
+  static constexpr int kStages = NSPLIT == 2 ? 4 : 3;
   static constexpr int kChunk = kBwdBK * 128;                    // 64 slots x BK rows = 4 KB
-  static constexpr int kA = 2 * kChunk;                          // 128 slots
-  static constexpr int kB = 4 * kChunk;                          // 256 slots
+  static constexpr int kA = 2 * kChunk;                          // this CTA's 128 P slots
+  static constexpr int kB = (kBwdHalfN / 64) * kChunk;           // this CTA's Q slots
   // stage: O_P | R_P[i] | O_Q | R_Q[i]
   static constexpr int kOffOP = 0;
   static constexpr int kOffRP = kA;
@@ -514,27 +521,30 @@ struct BwdSmem {
 // G = O^T R on all tiles, written directly only, self blocks included (the
 // true partial derivatives, for gradient checks and autograd).
 template <int NSPLIT, bool SYM>
-__global__ void __launch_bounds__(kBwdThreads, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kBwdThreads, 1)
     tc_backward_kernel(const __grid_constant__ BwdMaps maps, BwdArgs args) {
   using SM = BwdSmem<NSPLIT>;
   constexpr int kStages = SM::kStages;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = align1024(smem_raw);
+  // full[] and tempty[] are used in the leader only; empty[] and tfull[] in both
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + SM::kBarOff);
   uint64_t *empty = full + kStages;
   uint64_t *tfull = empty + kStages;
-  uint64_t *tempty = tfull + 2;
-  uint64_t *drain = tempty + 2;
+  uint64_t *tempty = tfull + kBwdBufs;
+  uint64_t *drain = tempty + kBwdBufs;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
   int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
   const int n_tiles = args.n_tiles;
   const int k_blocks = args.Npad / kBwdBK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
-    for (int a = 0; a < 2; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 8); }
+    for (int a = 0; a < kBwdBufs; ++a) { mbar_init(&tfull[a], 1); mbar_init(&tempty[a], 16); }
     mbar_init(drain, 1);
     *abort_flag = 0;
     fence_mbar_init();
@@ -543,18 +553,19 @@ __global__ void __launch_bounds__(kBwdThreads, 1)
     prefetch_tmap(&maps.o);
     for (int i = 0; i < NSPLIT; ++i) prefetch_tmap(&maps.r[i]);
   }
-  if (warp == 1) { tmem_alloc(tmem_slot, 512); tmem_relinquish(); }
+  if (warp == 1) { tmem_alloc_pair(tmem_slot, 512); tmem_relinquish_pair(); }
   tc_fence_before();
-  __syncthreads();
+  cluster_sync();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
   if (warp == 0) {
     if (lane == 0) {
       uint32_t it = 0;
-      for (int tile = blockIdx.x; tile < n_tiles && !aborted(abort_flag); tile += gridDim.x) {
+      for (int tile = pair; tile < n_tiles && !aborted(abort_flag); tile += npairs) {
         const int2 pq = args.tiles[tile];
-        const int xP = pq.x * kBwdBM, xQ = pq.y * kBwdBN;
+        const int xP = pq.x * kBwdPairM + (int)rank * kBwdBM;
+        const int xQ = pq.y * kBwdBN + (int)rank * kBwdHalfN;
         for (int kb = 0; kb < k_blocks; ++kb, ++it) {
           const int stage = it % kStages;
           const uint32_t round = it / kStages;
@@ -564,42 +575,48 @@ __global__ void __launch_bounds__(kBwdThreads, 1)
           }
           uint8_t *st = smem + stage * SM::kStage;
           const int y = kb * kBwdBK;
-          mbar_arrive_expect_tx(&full[stage],
-                                SYM ? SM::kStage : SM::kA + NSPLIT * SM::kB);
+          const uint32_t fb = mapa_shared(smem_u32(&full[stage]), 0);
+          if (rank == 0)
+            mbar_arrive_expect_tx(&full[stage],
+                                  2 * (SYM ? SM::kStage : SM::kA + NSPLIT * SM::kB));
           for (int c = 0; c < 2; ++c)
-            tma_load_2d(st + SM::kOffOP + c * SM::kChunk, &maps.o, &full[stage], xP + 64 * c, y);
+            tma_load_2d_pair(st + SM::kOffOP + c * SM::kChunk, &maps.o, fb, xP + 64 * c, y);
           if (SYM) {
             for (int i = 0; i < NSPLIT; ++i)
               for (int c = 0; c < 2; ++c)
-                tma_load_2d(st + SM::kOffRP + i * SM::kA + c * SM::kChunk, &maps.r[i],
-                            &full[stage], xP + 64 * c, y);
-            for (int c = 0; c < 4; ++c)
-              tma_load_2d(st + SM::kOffOQ + c * SM::kChunk, &maps.o, &full[stage], xQ + 64 * c, y);
+                tma_load_2d_pair(st + SM::kOffRP + i * SM::kA + c * SM::kChunk, &maps.r[i], fb,
+                                 xP + 64 * c, y);
+            for (int c = 0; c < kBwdHalfN / 64; ++c)
+              tma_load_2d_pair(st + SM::kOffOQ + c * SM::kChunk, &maps.o, fb, xQ + 64 * c, y);
           }
           for (int i = 0; i < NSPLIT; ++i)
-            for (int c = 0; c < 4; ++c)
-              tma_load_2d(st + SM::kOffRQ + i * SM::kB + c * SM::kChunk, &maps.r[i], &full[stage],
-                          xQ + 64 * c, y);
+            for (int c = 0; c < kBwdHalfN / 64; ++c)
+              tma_load_2d_pair(st + SM::kOffRQ + i * SM::kB + c * SM::kChunk, &maps.r[i], fb,
+                               xQ + 64 * c, y);
         }
       }
+      // drain (as in tc_forward): the leader's full barriers count both CTAs'
+      // bytes; the other CTA waits for the MMA's release of its last stages
       const uint32_t issued = it;
-      for (uint32_t r = (issued > (uint32_t)kStages ? issued - kStages : 0); r < issued; ++r)
-        if (!mbar_wait(&full[r % kStages], (r / kStages) & 1)) {
+      for (uint32_t r = (issued > (uint32_t)kStages ? issued - kStages : 0); r < issued; ++r) {
+        const bool ok = rank == 0 ? mbar_wait(&full[r % kStages], (r / kStages) & 1)
+                                  : mbar_wait(&empty[r % kStages], (r / kStages) & 1);
+        if (!ok) {
           record_error(args.status, kErrBwdTimeout, abort_flag);
           break;
         }
+      }
     }
   } else if (warp == 1) {
-    if (lane == 0) {
-      constexpr uint32_t idesc = idesc_bf16_f32(kBwdBM, kBwdBN, 1, 1);
+    if (lane == 0 && rank == 0) {
+      constexpr uint32_t idesc = idesc_bf16_f32(kBwdPairM, kBwdBN, 1, 1);
       uint32_t it = 0;
-      uint32_t chunk = 0;  // chunks issued by this CTA, across tiles
+      uint32_t chunk = 0;  // chunks issued by this pair, across tiles
       bool ok = true;
-      for (int tile = blockIdx.x; tile < n_tiles && ok && !aborted(abort_flag);
-           tile += gridDim.x) {
+      for (int tile = pair; tile < n_tiles && ok && !aborted(abort_flag); tile += npairs) {
         for (int kb0 = 0; kb0 < k_blocks && ok; kb0 += kBwdChunkKB, ++chunk) {
-          const int buf = chunk & 1;
-          const uint32_t use = chunk >> 1;
+          const int buf = chunk % kBwdBufs;
+          const uint32_t use = chunk / kBwdBufs;
           if (!mbar_wait(&tempty[buf], (use & 1) ^ 1)) {
             record_error(args.status, kErrBwdTimeout, abort_flag);
             ok = false;
@@ -627,24 +644,24 @@ __global__ void __launch_bounds__(kBwdThreads, 1)
               for (int i = 0; i < NSPLIT; ++i) {
                 const uint64_t dRQ =
                     sdesc_sw128(s0 + SM::kOffRQ + i * SM::kB + ko, SM::kChunk, 1024);
-                umma_bf16(d, dOP, dRQ, idesc, ((kb - kb0) | k16 | i) != 0);
+                umma_bf16_pair(d, dOP, dRQ, idesc, ((kb - kb0) | k16 | i) != 0);
               }
               if (SYM) {
 #pragma unroll
                 for (int i = 0; i < NSPLIT; ++i) {
                   const uint64_t dRP =
                       sdesc_sw128(s0 + SM::kOffRP + i * SM::kA + ko, SM::kChunk, 1024);
-                  umma_bf16(d, dRP, dOQ, idesc, 1);
+                  umma_bf16_pair(d, dRP, dOQ, idesc, 1);
                 }
               }
             }
-            umma_commit(&empty[stage]);
+            umma_commit_pair(&empty[stage], 0x3);
           }
           if (!ok) break;
-          umma_commit(&tfull[buf]);
+          umma_commit_pair(&tfull[buf], 0x3);
         }
       }
-      umma_commit(drain);
+      umma_commit_pair(drain, 0x1);
       if (!mbar_wait(drain, 0)) record_error(args.status, kErrBwdTimeout, abort_flag);
     }
   } else {
@@ -666,13 +683,13 @@ __global__ void __launch_bounds__(kBwdThreads, 1)
     float *Tb = reinterpret_cast<float *>(smem + SM::kTOff) + (warp - 2) * 32 * 9;
     uint32_t chunk = 0;
     bool ok = true;
-    for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
-      float accv[128];
+    for (int tile = pair; tile < n_tiles && ok; tile += npairs) {
+      float accv[kBwdHalfN];
 #pragma unroll
-      for (int i = 0; i < 128; ++i) accv[i] = 0.0f;
+      for (int i = 0; i < kBwdHalfN; ++i) accv[i] = 0.0f;
       for (int kb0 = 0; kb0 < k_blocks; kb0 += kBwdChunkKB, ++chunk) {
-        const int buf = chunk & 1;
-        const uint32_t use = chunk >> 1;
+        const int buf = chunk % kBwdBufs;
+        const uint32_t use = chunk / kBwdBufs;
         const bool w_ok = mbar_wait(&tfull[buf], use & 1);
         if (__any_sync(0xffffffffu, !w_ok)) {
           if (lane == 0) record_error(args.status, kErrBwdTimeout, abort_flag);
@@ -681,9 +698,9 @@ __global__ void __launch_bounds__(kBwdThreads, 1)
         }
         tc_fence_after();
         const uint32_t taddr =
-            tmem_base + buf * kBwdBN + half * 128 + ((uint32_t)(q * 32) << 16);
+            tmem_base + buf * kBwdBN + half * kBwdHalfN + ((uint32_t)(q * 32) << 16);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
+        for (int c = 0; c < kBwdHalfN / 32; ++c) {
           uint32_t v[32];
           __syncwarp();
           tmem_ld32(taddr + c * 32, v);
@@ -693,21 +710,24 @@ __global__ void __launch_bounds__(kBwdThreads, 1)
         }
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&tempty[buf]);
+        if (lane == 0) mbar_arrive_cluster(mapa_shared(smem_u32(&tempty[buf]), 0));
       }
       if (!ok) break;
 
       const int2 pq = args.tiles[tile];
-      const int rowbase = pq.x * kBwdBM + q * 32;
+      const int rowbase = pq.x * kBwdPairM + (int)rank * kBwdBM + q * 32;
       const int s1 = rowbase + lane;
       const int t1 = s1 / kGroupSlots, r1 = s1 % kGroupSlots;
       const int b = r1 / kGroupCols, k = t1 * kGroupCols + r1 % kGroupCols;
       const bool valid1 = r1 < kGroupUsed && k < L;
       const long long colt = (long long)b * L + k;  // transposed: + ((a*L+j)*32)*L
-      const int sQ = pq.y * kBwdBN + half * 128;
-      // 16 rounds of 8 columns through the transpose buffer Tb[row][col]
+      // columns: Q block pq.y of kBwdBN slots, inside slot group tQ from slot rQ
+      const int tQ = pq.y * kBwdBN / kGroupSlots;
+      const int rQ = pq.y * kBwdBN % kGroupSlots + half * kBwdHalfN;
+      const int sQ = tQ * kGroupSlots + rQ;
+      // 8 rounds of 8 columns through the transpose buffer Tb[row][col]
 #pragma unroll
-      for (int cb = 0; cb < 16; ++cb) {
+      for (int cb = 0; cb < kBwdHalfN / 8; ++cb) {
         __syncwarp();
 #pragma unroll
         for (int e = 0; e < 8; ++e) Tb[lane * 9 + e] = accv[cb * 8 + e];
@@ -716,9 +736,9 @@ __global__ void __launch_bounds__(kBwdThreads, 1)
         if (SYM) {
 #pragma unroll 1
           for (int col = 0; col < 8; ++col) {
-            const int r2 = half * 128 + cb * 8 + col;
+            const int r2 = rQ + cb * 8 + col;
             const int s2 = sQ + cb * 8 + col;
-            const int a = r2 / kGroupCols, j = pq.y * kGroupCols + r2 % kGroupCols;
+            const int a = r2 / kGroupCols, j = tQ * kGroupCols + r2 % kGroupCols;
             const bool valid2 = r2 < kGroupUsed && j < L;
             if (s1 < s2) {
               const float val = Tb[lane * 9 + col];
@@ -732,9 +752,9 @@ __global__ void __launch_bounds__(kBwdThreads, 1)
         }
         // (B) direct writes and the ones-slot row: lanes = 4 rows x 8 columns
         const int col = lane & 7;
-        const int r2 = half * 128 + cb * 8 + col;
+        const int r2 = rQ + cb * 8 + col;
         const int s2 = sQ + cb * 8 + col;
-        const int a = r2 / kGroupCols, j = pq.y * kGroupCols + r2 % kGroupCols;
+        const int a = r2 / kGroupCols, j = tQ * kGroupCols + r2 % kGroupCols;
         const bool valid2 = r2 < kGroupUsed && j < L;
 #pragma unroll
         for (int it = 0; it < 8; ++it) {
@@ -755,11 +775,11 @@ __global__ void __launch_bounds__(kBwdThreads, 1)
   }
 
   tc_fence_before();
-  __syncthreads();
+  cluster_sync();
   if (warp == 1) {
     __syncwarp();
     tc_fence_after();
-    tmem_dealloc(tmem_base, 512);
+    tmem_dealloc_pair(tmem_base, 512);
   }
 }
 
@@ -836,13 +856,13 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
   ba.x2 = x2; ba.g2 = g2; ba.g1d = c->d_g1d; ba.tiles = c->d_bwd_tiles;
   ba.n_tiles = c->n_bwd_tiles; ba.status = c->d_status; ba.L = L; ba.S = c->S; ba.Npad = c->Npad;
   ba.lambda_pair = c->lambda_pair;
-  const int bwd_grid = c->n_bwd_tiles < c->num_sms ? c->n_bwd_tiles : c->num_sms;
+  const int bwd_pairs = c->n_bwd_tiles < c->bwd_pairs ? c->n_bwd_tiles : c->bwd_pairs;
   if (c->gradient == CCM_GRADIENT_PARTIAL)
-    tc_backward_kernel<NSPLIT, false><<<bwd_grid, kBwdThreads, BwdSmem<NSPLIT>::kTotal, c->stream>>>(
-        c->bwd_maps, ba);
+    tc_backward_kernel<NSPLIT, false>
+        <<<2 * bwd_pairs, kBwdThreads, BwdSmem<NSPLIT>::kTotal, c->stream>>>(c->bwd_maps, ba);
   else
-    tc_backward_kernel<NSPLIT, true><<<bwd_grid, kBwdThreads, BwdSmem<NSPLIT>::kTotal, c->stream>>>(
-        c->bwd_maps, ba);
+    tc_backward_kernel<NSPLIT, true>
+        <<<2 * bwd_pairs, kBwdThreads, BwdSmem<NSPLIT>::kTotal, c->stream>>>(c->bwd_maps, ba);
   prof_mark(c);
 
   FinalizeArgs za{};
@@ -854,6 +874,19 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
   prof_mark(c);
   count_launch(c, 4);
   return cudaGetLastError();
+}
+
+cudaError_t tc_backward_max_pairs(int nsplit, int *pairs) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2, 1, 1);
+  cfg.blockDim = dim3(kBwdThreads, 1, 1);
+  cfg.dynamicSmemBytes = nsplit == 3 ? BwdSmem<3>::kTotal : BwdSmem<2>::kTotal;
+  int n = 0;
+  cudaError_t e = nsplit == 3
+                      ? cudaOccupancyMaxActiveClusters(&n, tc_backward_kernel<3, true>, &cfg)
+                      : cudaOccupancyMaxActiveClusters(&n, tc_backward_kernel<2, true>, &cfg);
+  *pairs = n;
+  return e;
 }
 
 cudaError_t tc_forward_max_pairs(int nsplit, int *pairs) {
