@@ -204,6 +204,13 @@ __device__ __forceinline__ bool named_bar_or(int id, int nthreads, bool pred) {
   return r != 0;
 }
 
+// 32-byte global store (one full sector); `p` must be 32-byte aligned.
+__device__ __forceinline__ void st_global_v8(void *p, const uint32_t (&r)[8]) {
+  asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "r"(r[0]), "r"(r[1]),
+               "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+               : "memory");
+}
+
 // ------------------------------------------------------- CTA pairs (clusters of 2)
 // A pair of CTAs (cluster ranks 0 and 1) shares one tcgen05 MMA of M = 256:
 // each CTA holds half of A (its 128 rows) and half of B (128 of the N columns)

@@ -258,14 +258,15 @@ __device__ __forceinline__ void fwd_epilogue_tile(const FwdArgs &args, uint32_t 
     tmem_ld32(taddr + cc * 32, v);
     tmem_wait_ld();
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      uint32_t ph[4], pl[4], pl2[4];
+    for (int u = 0; u < 2; ++u) {
+      // 16 columns = 32 bytes of each bf16 term: one full-sector store per term
+      uint32_t ph[8], pl[8], pl2[8];
 #pragma unroll
-      for (int e2 = 0; e2 < 4; ++e2) {
+      for (int e2 = 0; e2 < 8; ++e2) {
         uint32_t hh = 0, ll = 0, l2 = 0;
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-          const int i = u * 8 + e2 * 2 + e;
+          const int i = u * 16 + e2 * 2 + e;
           const int col = cc * 32 + i;
           float r = 0.0f;
           if (col < kGroupUsed) {
@@ -284,11 +285,10 @@ __device__ __forceinline__ void fwd_epilogue_tile(const FwdArgs &args, uint32_t 
         }
         ph[e2] = hh; pl[e2] = ll; pl2[e2] = l2;
       }
-      const long long off = rbase + cc * 32 + u * 8;
-      *reinterpret_cast<uint4 *>(args.r[0] + off) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
-      *reinterpret_cast<uint4 *>(args.r[1] + off) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
-      if (NSPLIT > 2)
-        *reinterpret_cast<uint4 *>(args.r[2] + off) = make_uint4(pl2[0], pl2[1], pl2[2], pl2[3]);
+      const long long off = rbase + cc * 32 + u * 16;
+      st_global_v8(args.r[0] + off, ph);
+      st_global_v8(args.r[1] + off, pl);
+      if (NSPLIT > 2) st_global_v8(args.r[2] + off, pl2);
     }
   }
   // loss partial, one per (tile, epilogue warp), summed in fixed order by tc_finalize
