@@ -423,6 +423,15 @@ def main():
         dom_ms = kernels.get(dom, float("nan"))
         achieved = flops / (dom_ms / 1e3) / 1e12
         traffic = traffic_from_profiles(dom)
+        # tensor-core flops actually issued by the dominant kernel: every split term,
+        # the padded shapes (S = 256 slots per 12 columns, rows padded to 256) and,
+        # for the backward, both products O^T R and R^T O on the upper-triangle tiles
+        nsplit = 3 if args.path == "tc_bf16x3" else 2
+        T = (L + 11) // 12
+        S, Npad = 256 * T, (N + 255) // 256 * 256
+        executed = {"tc_forward": 2.0 * Npad * S * S * nsplit,
+                    "tc_backward": T * (T + 1) / 2 * 256 * 256 * 2.0 * Npad * 2 * nsplit}[dom]
+        executed_tf = executed / (dom_ms / 1e3) / 1e12
 
         plain = None
         if args.plain_steps > 0 and world == 1:
@@ -472,7 +481,9 @@ def main():
             "roofline": {"bound": "tensor", "kernel": dom, "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} bf16_tflops_sustained",
-                         "flops_per_launch": flops, "traffic": traffic},
+                         "flops_per_launch": flops, "traffic": traffic,
+                         "executed_flops_per_launch": executed,
+                         "executed_tflops": executed_tf, "executed_frac": executed_tf / peak},
             "kernels_ms_per_launch": kernels,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes,
