@@ -58,7 +58,7 @@ def calculate_weights(msa: np.ndarray, threshold: float = 0.8, device: int = 0) 
 
 def solve_batch(msas, workers: int = 8, path: str = "tc_bf16x2", threshold: float = 0.8,
                 max_iterations: int = 250, epsilon: float = 0.01, contact_maps: bool = True,
-                device: int = 0):
+                device: int = 0, sms_per_worker: int = 0):
     """Solve many alignments to convergence concurrently (ccm_solve_batch).
 
     Returns (results, maps): per-alignment CcmBatchResult and APC contact maps."""
@@ -71,6 +71,7 @@ def solve_batch(msas, workers: int = 8, path: str = "tc_bf16x2", threshold: floa
     p = _lib.CcmBatchParams()
     lib().ccm_batch_params_default(ctypes.byref(p))
     p.workers, p.path, p.reweighting_threshold, p.device = workers, PATHS[path], threshold, device
+    p.sms_per_worker = sms_per_worker
     p.cg.max_iterations, p.cg.epsilon = max_iterations, epsilon
     res = (_lib.CcmBatchResult * max(n, 1))()
     maps = [np.empty((a.shape[1], a.shape[1]), dtype=np.float32) for a in arrs] if contact_maps else None
@@ -88,13 +89,14 @@ class Evaluator:
 
     ``path`` is one of ``tc_bf16x2`` (default), ``tc_bf16x3``, ``simt_f32``, ``simt_f64``;
     ``gradient`` is ``tied`` (the reference's g, default) or ``partial`` (true
-    partial derivatives, as autograd needs them).
+    partial derivatives, as autograd needs them); ``max_sms`` > 0 confines the
+    tensor-core kernels to that many SMs (for contexts that share one GPU).
     """
 
     def __init__(self, msa: np.ndarray, weights: Optional[np.ndarray] = None,
                  lambda_single: float = 0.01, lambda_pair: Optional[float] = None,
                  path: str = "tc_bf16x2", device: int = 0, stream: Optional[int] = None,
-                 gradient: str = "tied"):
+                 gradient: str = "tied", max_sms: int = 0):
         self._ctx = ctypes.c_void_p(None)
         self.msa = np.ascontiguousarray(msa, dtype=np.uint8)
         self.N, self.L = self.msa.shape
@@ -102,7 +104,10 @@ class Evaluator:
         self.nvar = nvar_padded(self.L)
         self.nsp = nsingle_padded(self.L)
         self.lambda_single = float(lambda_single)
-        self.lambda_pair = float(0.2 * (self.L - 1) if lambda_pair is None else lambda_pair)
+        # default as the reference computes it, in float: 0.2f * (L - 1)
+        # (src/ccmpred.c:224,502-503)
+        self.lambda_pair = float(np.float32(0.2) * np.float32(self.L - 1)
+                                 if lambda_pair is None else lambda_pair)
         opt = _lib.CcmOptions()
         lib().ccm_options_default(ctypes.byref(opt), self.L)
         opt.lambda_single = self.lambda_single
@@ -111,6 +116,7 @@ class Evaluator:
         opt.device = device
         opt.stream = stream
         opt.gradient = _lib.GRADIENTS[gradient]
+        opt.max_sms = max_sms
         self.gradient = gradient
         wptr = None
         if weights is not None:

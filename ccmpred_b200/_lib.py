@@ -35,7 +35,7 @@ GRADIENTS = {"tied": GRADIENT_TIED, "partial": GRADIENT_PARTIAL}
 class CcmOptions(ctypes.Structure):
     _fields_ = [("lambda_single", ctypes.c_float), ("lambda_pair", ctypes.c_float),
                 ("path", ctypes.c_int), ("device", ctypes.c_int), ("stream", ctypes.c_void_p),
-                ("gradient", ctypes.c_int), ("pad", ctypes.c_int)]
+                ("gradient", ctypes.c_int), ("max_sms", ctypes.c_int)]
 
 
 class CcmResult(ctypes.Structure):
@@ -80,7 +80,7 @@ class CcmBatchParams(ctypes.Structure):
     _fields_ = [("reweighting_threshold", ctypes.c_float), ("lambda_single", ctypes.c_float),
                 ("lambda_pair_factor", ctypes.c_float), ("path", ctypes.c_int),
                 ("workers", ctypes.c_int), ("device", ctypes.c_int), ("use_apc", ctypes.c_int),
-                ("pad", ctypes.c_int), ("cg", CcmCgParams)]
+                ("sms_per_worker", ctypes.c_int), ("cg", CcmCgParams)]
 
 
 class CcmBatchResult(ctypes.Structure):
@@ -141,6 +141,8 @@ SIGNATURES = {
                                        ctypes.POINTER(ctypes.c_size_t)]),
     "ccm_init_bias": (None, [_u8p, ctypes.c_int, ctypes.c_int, _f32p]),
     "ccm_sum_submatrices": (ctypes.c_double, [_f32p, _f32p, ctypes.c_int]),
+    "ccm_sum_submatrices_gpu": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                               ctypes.c_void_p]),
     "ccm_apc": (None, [_f32p, ctypes.c_int]),
     "ccm_normalize": (ctypes.c_int, [_f32p, ctypes.c_int]),
     "ccm_write_matrix": (ctypes.c_int, [ctypes.c_char_p, _f32p, ctypes.c_int, ctypes.c_int]),

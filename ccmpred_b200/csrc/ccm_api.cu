@@ -1,5 +1,6 @@
 // C ABI of libccmpred_b200.so: context lifecycle, evaluation dispatch and the
 // reference-compatible backend triples.  See include/ccmpred_b200.h.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -22,6 +23,41 @@ void prof_mark(ccm_context *c) {
 }
 
 void count_launch(ccm_context *c, int n) { c->launches += n; }
+
+cudaError_t dev_alloc_raw(ccm_context *c, void **p, size_t bytes) {
+  return c->pool ? cudaMallocFromPoolAsync(p, bytes, c->pool, c->stream)
+                 : cudaMallocAsync(p, bytes, c->stream);
+}
+
+// Small pinned host records (a context's result, the CG's step scalars) come
+// from one process-wide slab of 256-byte slots that is never returned to CUDA:
+// cudaFreeHost waits for the whole device, which would stall the streams of
+// every other context at each context tear-down.
+static constexpr size_t kPinnedSlot = 256;
+static constexpr size_t kPinnedChunk = 256 * kPinnedSlot;
+static std::mutex pinned_mutex;
+static std::vector<void *> pinned_free;
+
+void *pinned_small_alloc(size_t bytes) {
+  if (bytes > kPinnedSlot) return nullptr;
+  std::lock_guard<std::mutex> lock(pinned_mutex);
+  if (pinned_free.empty()) {
+    void *chunk = nullptr;
+    if (cudaHostAlloc(&chunk, kPinnedChunk, cudaHostAllocPortable) != cudaSuccess) return nullptr;
+    for (size_t i = kPinnedChunk / kPinnedSlot; i-- > 0;)
+      pinned_free.push_back(static_cast<char *>(chunk) + i * kPinnedSlot);
+  }
+  void *p = pinned_free.back();
+  pinned_free.pop_back();
+  std::memset(p, 0, kPinnedSlot);
+  return p;
+}
+
+void pinned_small_free(void *p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lock(pinned_mutex);
+  pinned_free.push_back(p);
+}
 
 int set_last_error(int code, const char *fmt, ...);
 
@@ -126,6 +162,14 @@ __global__ void build_onehot_kernel(const uint8_t *__restrict__ msa, __nv_bfloat
   O[idx] = __float2bfloat16_rn(v);
 }
 
+// Device memory of a context is allocated and freed stream-ordered on the
+// context's stream.  Plain cudaFree waits for the whole device, which in the
+// batch solver would stall every other worker's stream at each alignment.
+template <class T>
+cudaError_t dev_alloc(ccm_context *c, T **p, size_t bytes) {
+  return dev_alloc_raw(c, reinterpret_cast<void **>(p), bytes);
+}
+
 bool configured[64] = {false};
 std::mutex configure_mutex;
 
@@ -145,17 +189,17 @@ int alloc_tc(ccm_context *c) {
   // rows padded to the forward's 256-row CTA-pair tiles
   c->Npad = ((c->N + 255) / 256) * 256;
   const size_t S = c->S, Np = c->Npad;
-  CCM_CUDA_TRY(cudaMalloc(&c->d_onehot, sizeof(__nv_bfloat16) * Np * S));
+  CCM_CUDA_TRY(dev_alloc(c, &c->d_onehot, sizeof(__nv_bfloat16) * Np * S));
   for (int i = 0; i < c->nsplit; ++i) {
-    CCM_CUDA_TRY(cudaMalloc(&c->d_wperm[i], sizeof(__nv_bfloat16) * S * S));
+    CCM_CUDA_TRY(dev_alloc(c, &c->d_wperm[i], sizeof(__nv_bfloat16) * S * S));
     CCM_CUDA_TRY(cudaMemsetAsync(c->d_wperm[i], 0, sizeof(__nv_bfloat16) * S * S, c->stream));
-    CCM_CUDA_TRY(cudaMalloc(&c->d_r[i], sizeof(__nv_bfloat16) * Np * S));
+    CCM_CUDA_TRY(dev_alloc(c, &c->d_r[i], sizeof(__nv_bfloat16) * Np * S));
     CCM_CUDA_TRY(cudaMemsetAsync(c->d_r[i], 0, sizeof(__nv_bfloat16) * Np * S, c->stream));
   }
   const long long fwd_tiles = (long long)(c->Npad / 128) * c->T;
-  CCM_CUDA_TRY(cudaMalloc(&c->d_part_f, sizeof(double) * fwd_tiles * 8));
-  CCM_CUDA_TRY(cudaMalloc(&c->d_part_reg, sizeof(double) * kQ * c->L));
-  CCM_CUDA_TRY(cudaMalloc(&c->d_g1d, sizeof(float) * (kQ - 1) * c->L));
+  CCM_CUDA_TRY(dev_alloc(c, &c->d_part_f, sizeof(double) * fwd_tiles * 8));
+  CCM_CUDA_TRY(dev_alloc(c, &c->d_part_reg, sizeof(double) * kQ * c->L));
+  CCM_CUDA_TRY(dev_alloc(c, &c->d_g1d, sizeof(float) * (kQ - 1) * c->L));
 
   std::vector<int2> tiles;
   // P and Q in 256-slot blocks (rows, columns of C); the symmetric gradient
@@ -164,7 +208,7 @@ int alloc_tc(ccm_context *c) {
     for (int P = 0; P < c->T; ++P)
       if (c->gradient == CCM_GRADIENT_PARTIAL || P <= Q) tiles.push_back(make_int2(P, Q));
   c->n_bwd_tiles = (int)tiles.size();
-  CCM_CUDA_TRY(cudaMalloc(&c->d_bwd_tiles, sizeof(int2) * tiles.size()));
+  CCM_CUDA_TRY(dev_alloc(c, &c->d_bwd_tiles, sizeof(int2) * tiles.size()));
   CCM_CUDA_TRY(cudaMemcpyAsync(c->d_bwd_tiles, tiles.data(), sizeof(int2) * tiles.size(),
                                cudaMemcpyHostToDevice, c->stream));
 
@@ -187,21 +231,22 @@ int alloc_tc(ccm_context *c) {
 
 int alloc_simt(ccm_context *c, size_t elem) {
   const size_t QL = (size_t)kQ * c->L;
-  CCM_CUDA_TRY(cudaMalloc(&c->d_simt_pc, elem * (size_t)c->N * QL));
-  CCM_CUDA_TRY(cudaMalloc(&c->d_simt_g2, elem * QL * QL));
-  CCM_CUDA_TRY(cudaMalloc(&c->d_simt_g1, elem * (size_t)(kQ - 1) * c->L));
-  CCM_CUDA_TRY(cudaMalloc(&c->d_simt_part, sizeof(double) * ((size_t)c->N + QL)));
+  CCM_CUDA_TRY(dev_alloc(c, &c->d_simt_pc, elem * (size_t)c->N * QL));
+  CCM_CUDA_TRY(dev_alloc(c, &c->d_simt_g2, elem * QL * QL));
+  CCM_CUDA_TRY(dev_alloc(c, &c->d_simt_g1, elem * (size_t)(kQ - 1) * c->L));
+  CCM_CUDA_TRY(dev_alloc(c, &c->d_simt_part, sizeof(double) * ((size_t)c->N + QL)));
   return CCM_OK;
 }
 
 void free_all(ccm_context *c) {
-  auto f = [](void *p) { if (p) cudaFree(p); };
+  // stream-ordered frees: cudaFree would wait for every stream of the device
+  auto f = [c](void *p) { if (p) cudaFreeAsync(p, c->stream); };
   f(c->d_msa); f(c->d_w); f(c->d_out); f(c->d_onehot);
   for (int i = 0; i < 3; ++i) { f(c->d_wperm[i]); f(c->d_r[i]); }
   f(c->d_part_f); f(c->d_part_reg); f(c->d_g1d); f(c->d_bwd_tiles);
   f(c->d_simt_pc); f(c->d_simt_g2); f(c->d_simt_part); f(c->d_simt_g1);
   f(c->d_xh); f(c->d_gh);
-  if (c->h_out) cudaFreeHost(c->h_out);
+  if (c->h_out) pinned_small_free(c->h_out);
   std::free(c->h_w);
   if (c->prof_events) {
     for (int i = 0; i < c->prof_max * kMaxProfMarks; ++i) cudaEventDestroy(c->prof_events[i]);
@@ -299,27 +344,8 @@ int init_backend(ccm_userdata *ud) {
 
 }  // namespace
 
-extern "C" {
-
-const char *ccm_last_error(void) { return g_last_error; }
-
-void ccm_set_default_path(int path) { g_default_path = path; }
-
-long long ccm_nsingle_padded(int ncol) { return nsingle_padded_of(ncol); }
-long long ccm_nvar_padded(int ncol) { return nvar_padded_of(ncol); }
-
-void ccm_options_default(ccm_options *opt, int ncol) {
-  if (!opt) return;
-  opt->lambda_single = 0.01f;
-  opt->lambda_pair = 0.2f * (float)(ncol - 1);
-  opt->path = CCM_PATH_TC_BF16X2;
-  opt->device = 0;
-  opt->stream = nullptr;
-  opt->gradient = CCM_GRADIENT_TIED;
-}
-
-int ccm_create(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
-               const float *weights, const ccm_options *opt) {
+int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
+                        const float *weights, const ccm_options *opt, cudaMemPool_t pool) {
   if (!out || !msa || ncol <= 0 || nrow <= 0)
     return set_error(CCM_ERR_INVALID, "ccm_create: invalid arguments");
   *out = nullptr;
@@ -345,6 +371,7 @@ int ccm_create(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
   if (rc != CCM_OK) return rc;
 
   ccm_context *c = new ccm_context();
+  c->pool = pool;
   c->device = o.device;
   c->num_sms = prop.multiProcessorCount;
   if (o.path == CCM_PATH_TC_BF16X2 || o.path == CCM_PATH_TC_BF16X3) {
@@ -354,6 +381,11 @@ int ccm_create(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
     if (e != cudaSuccess || c->fwd_pairs < 1 || c->bwd_pairs < 1) {
       delete c;
       return set_error(CCM_ERR_CUDA, "tc_forward cluster occupancy: %s", cudaGetErrorString(e));
+    }
+    if (o.max_sms > 0) {
+      const int pairs = std::max(1, o.max_sms / 2);
+      c->fwd_pairs = std::min(c->fwd_pairs, pairs);
+      c->bwd_pairs = std::min(c->bwd_pairs, pairs);
     }
   }
   c->path = o.path;
@@ -386,13 +418,14 @@ int ccm_create(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
   c->h_w = static_cast<float *>(std::malloc(sizeof(float) * nrow));
   if (!c->h_w) return fail(set_error(CCM_ERR_NOMEM, "host weights"));
   for (int i = 0; i < nrow; ++i) c->h_w[i] = weights ? weights[i] : 1.0f;
-  CCM_CTX_TRY(cudaMalloc(&c->d_msa, (size_t)ncol * nrow));
+  CCM_CTX_TRY(dev_alloc(c, &c->d_msa, (size_t)ncol * nrow));
   CCM_CTX_TRY(cudaMemcpyAsync(c->d_msa, msa, (size_t)ncol * nrow, cudaMemcpyHostToDevice, c->stream));
-  CCM_CTX_TRY(cudaMalloc(&c->d_w, sizeof(float) * nrow));
+  CCM_CTX_TRY(dev_alloc(c, &c->d_w, sizeof(float) * nrow));
   CCM_CTX_TRY(cudaMemcpyAsync(c->d_w, c->h_w, sizeof(float) * nrow, cudaMemcpyHostToDevice, c->stream));
-  CCM_CTX_TRY(cudaMalloc(&c->d_out, sizeof(ccm_result)));
+  CCM_CTX_TRY(dev_alloc(c, &c->d_out, sizeof(ccm_result)));
   CCM_CTX_TRY(cudaMemsetAsync(c->d_out, 0, sizeof(ccm_result), c->stream));
-  CCM_CTX_TRY(cudaMallocHost(&c->h_out, sizeof(ccm_result)));
+  c->h_out = static_cast<ccm_result *>(pinned_small_alloc(sizeof(ccm_result)));
+  if (!c->h_out) return fail(set_error(CCM_ERR_NOMEM, "pinned result record"));
   c->d_status = &c->d_out->status;
 
   if (c->path == CCM_PATH_TC_BF16X2 || c->path == CCM_PATH_TC_BF16X3) {
@@ -405,6 +438,31 @@ int ccm_create(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
 #undef CCM_CTX_TRY
   *out = c;
   return CCM_OK;
+}
+
+extern "C" {
+
+const char *ccm_last_error(void) { return g_last_error; }
+
+void ccm_set_default_path(int path) { g_default_path = path; }
+
+long long ccm_nsingle_padded(int ncol) { return nsingle_padded_of(ncol); }
+long long ccm_nvar_padded(int ncol) { return nvar_padded_of(ncol); }
+
+void ccm_options_default(ccm_options *opt, int ncol) {
+  if (!opt) return;
+  opt->lambda_single = 0.01f;
+  opt->lambda_pair = 0.2f * (float)(ncol - 1);
+  opt->path = CCM_PATH_TC_BF16X2;
+  opt->device = 0;
+  opt->stream = nullptr;
+  opt->gradient = CCM_GRADIENT_TIED;
+  opt->max_sms = 0;
+}
+
+int ccm_create(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
+               const float *weights, const ccm_options *opt) {
+  return ccm::create_context(out, msa, ncol, nrow, weights, opt, nullptr);
 }
 
 int ccm_destroy(ccm_context *ctx) {
@@ -439,8 +497,8 @@ int ccm_evaluate_host(ccm_context *c, const float *x, float *g, long long nvar, 
     return set_error(CCM_ERR_INVALID, "ccm_evaluate_host: nvar %lld != nvar_padded %lld", nvar, c->nvarp);
   const size_t bytes = sizeof(float) * (size_t)nvar;
   if (!c->d_xh) {
-    CCM_CUDA_TRY(cudaMalloc(&c->d_xh, bytes));
-    CCM_CUDA_TRY(cudaMalloc(&c->d_gh, bytes));
+    CCM_CUDA_TRY(dev_alloc(c, &c->d_xh, bytes));
+    CCM_CUDA_TRY(dev_alloc(c, &c->d_gh, bytes));
   }
   CCM_CUDA_TRY(cudaMemcpyAsync(c->d_xh, x, bytes, cudaMemcpyHostToDevice, c->stream));
   int rc = enqueue_eval(c, c->d_xh, c->d_gh);

@@ -3,7 +3,12 @@
 // reweighting, init_bias, the device conjugate gradient and the APC contact
 // map.  Alignments are handed out largest-first (cost ~ N L^2) so that the
 // long solves start early.  Small alignments leave most of the GPU idle on
-// their own; running several at once on separate streams fills it.
+// their own; running several at once on separate streams fills it.  The
+// parameter vector x of each solve lives on the device only (the host sends
+// the 20 L single fields and receives the L x L contact map), device memory is
+// allocated and freed stream-ordered from one pool that keeps it mapped, and
+// pinned records come from a never-freed slab: no worker's set-up or tear-down
+// waits for the whole device or moves the full x over PCIe.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -31,7 +36,7 @@ void ccm_batch_params_default(ccm_batch_params *p) {
   p->workers = 8;
   p->device = 0;
   p->use_apc = 1;
-  p->pad = 0;
+  p->sms_per_worker = 0;
   ccm_cg_params_default(&p->cg);
 }
 
@@ -47,6 +52,27 @@ int ccm_solve_batch(int n, const ccm_msa_desc *msas, const ccm_batch_params *par
     const double cb = (double)msas[b].nrow * msas[b].ncol * msas[b].ncol;
     return ca > cb;
   });
+  const int nw = std::min(params->workers, std::max(n, 1));
+  // An optional share of the SMs for each worker's contexts.  Measured on B200,
+  // no share is faster: the prep and CG kernels spread over every SM anyway,
+  // so a share only shrinks the GEMM grids.
+  const int max_sms = params->sms_per_worker > 0 ? params->sms_per_worker : 0;
+  // One memory pool for the whole batch that keeps freed blocks mapped: each
+  // alignment's buffers reuse the previous alignment's memory instead of
+  // mapping fresh device memory (the default pool gives it back at every
+  // synchronisation).  Destroyed when the batch ends.
+  cudaMemPool_t pool = nullptr;
+  {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = params->device;
+    if (cudaSetDevice(params->device) != cudaSuccess || cudaMemPoolCreate(&pool, &props) != cudaSuccess)
+      return ccm::set_last_error(CCM_ERR_CUDA, "ccm_solve_batch: cannot create a memory pool");
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   std::atomic<int> next(0);
   std::atomic<int> first_error(CCM_OK);
   std::mutex err_mutex;
@@ -79,11 +105,14 @@ int ccm_solve_batch(int n, const ccm_msa_desc *msas, const ccm_batch_params *par
       if (params->reweighting_threshold < 1.0f)
         rc = ccm_calculate_weights(m.msa, L, N, params->reweighting_threshold, w.data(),
                                    params->device);
-      const long long nv = ccm_nvar_padded(L);
-      std::vector<float> x(rc == CCM_OK ? (size_t)nv : 0);
+      // x lives on the device only: the host computes the single fields of
+      // init_bias (20 L floats) and the couplings start at zero
+      const long long nv = ccm_nvar_padded(L), nsp = ccm_nsingle_padded(L);
+      std::vector<float> x1(rc == CCM_OK ? (size_t)nsp : 0, 0.0f);
       ccm_context *ctx = nullptr;
+      float *d_x = nullptr, *d_map = nullptr;
       if (rc == CCM_OK) {
-        ccm_init_bias(m.msa, L, N, x.data());
+        ccm::init_single_fields(m.msa, L, N, x1.data());
         ccm_options o;
         ccm_options_default(&o, L);
         o.lambda_single = params->lambda_single;
@@ -91,16 +120,35 @@ int ccm_solve_batch(int n, const ccm_msa_desc *msas, const ccm_batch_params *par
         o.path = params->path;
         o.device = params->device;
         o.stream = stream;
-        rc = ccm_create(&ctx, m.msa, L, N, w.data(), &o);
+        o.max_sms = max_sms;
+        rc = ccm::create_context(&ctx, m.msa, L, N, w.data(), &o, pool);
       }
+      auto cuda_ok = [&](cudaError_t e) {
+        if (e != cudaSuccess && rc == CCM_OK)
+          rc = ccm::set_last_error(CCM_ERR_CUDA, "ccm_solve_batch: %s", cudaGetErrorString(e));
+        return rc == CCM_OK;
+      };
+      if (rc == CCM_OK && cuda_ok(ccm::dev_alloc_raw(ctx, reinterpret_cast<void **>(&d_x),
+                                                      sizeof(float) * (size_t)nv)) &&
+          cuda_ok(cudaMemsetAsync(d_x + nsp, 0, sizeof(float) * (size_t)(nv - nsp), stream)))
+        cuda_ok(cudaMemcpyAsync(d_x, x1.data(), sizeof(float) * (size_t)nsp,
+                                cudaMemcpyHostToDevice, stream));
       ccm_cg_result cg;
       std::memset(&cg, 0, sizeof(cg));
-      if (rc == CCM_OK) rc = ccm_conjugrad_host(ctx, x.data(), nv, &params->cg, nullptr, nullptr, &cg);
-      if (ctx) ccm_destroy(ctx);
+      if (rc == CCM_OK) rc = ccm_conjugrad_gpu(ctx, d_x, nv, &params->cg, nullptr, nullptr, &cg);
       if (rc == CCM_OK && contact_maps && contact_maps[i]) {
-        ccm_sum_submatrices(x.data(), contact_maps[i], L);
-        if (params->use_apc) ccm_apc(contact_maps[i], L);
+        // contact scores on the device (bit-identical to the host sum_submatrices);
+        // only the L x L map comes back
+        const size_t mb = sizeof(float) * (size_t)L * L;
+        if (cuda_ok(ccm::dev_alloc_raw(ctx, reinterpret_cast<void **>(&d_map), mb)) &&
+            cuda_ok(ccm::launch_contact_scores(d_x, d_map, L, stream)) &&
+            cuda_ok(cudaMemcpyAsync(contact_maps[i], d_map, mb, cudaMemcpyDeviceToHost, stream)) &&
+            cuda_ok(cudaStreamSynchronize(stream)) && params->use_apc)
+          ccm_apc(contact_maps[i], L);
       }
+      if (d_map) cudaFreeAsync(d_map, stream);
+      if (d_x) cudaFreeAsync(d_x, stream);
+      if (ctx) ccm_destroy(ctx);
       r.status = rc == CCM_OK ? cg.status : rc;
       r.iterations = cg.iterations;
       r.evaluations = cg.evaluations;
@@ -116,10 +164,12 @@ int ccm_solve_batch(int n, const ccm_msa_desc *msas, const ccm_batch_params *par
     }
     cudaStreamDestroy(stream);
   };
-  const int nw = std::min(params->workers, std::max(n, 1));
   std::vector<std::thread> threads;
   for (int t = 0; t < nw; ++t) threads.emplace_back(work);
   for (auto &t : threads) t.join();
+  // every allocation has been freed on its worker's stream; the pool's memory
+  // is released once those frees have completed
+  cudaMemPoolDestroy(pool);
   const int rc = first_error.load();
   if (rc != CCM_OK) ccm::set_last_error(rc, "ccm_solve_batch: %s", err_text.c_str());
   return rc;

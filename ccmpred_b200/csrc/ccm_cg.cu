@@ -113,10 +113,12 @@ __global__ void cg_dots_final_kernel(const double *__restrict__ part, int nblock
   }
 }
 
-// s = -g + beta * s  (beta from device memory; beta == 0 gives steepest descent)
-__global__ void cg_direction_kernel(const float *__restrict__ g, const double *__restrict__ beta,
+// s = -g + beta * s  (beta == 0 gives steepest descent).  beta is a launch
+// argument: it is fixed when the kernel is enqueued, with no host buffer that
+// the host could overwrite before the copy runs.
+__global__ void cg_direction_kernel(const float *__restrict__ g, double beta,
                                     float *__restrict__ s, long long n) {
-  const float b = (float)beta[0];
+  const float b = (float)beta;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     s[i] = fmaf(b, s[i], -g[i]);
@@ -145,27 +147,27 @@ struct CgState {
   float *xb[2] = {nullptr, nullptr};  // x ping-pong (xb[0] may be the caller's x)
   float *gb[2] = {nullptr, nullptr};
   float *s = nullptr;
-  double *d_alpha = nullptr, *d_beta = nullptr, *d_part = nullptr, *d_dots = nullptr;
+  double *d_alpha = nullptr, *d_part = nullptr, *d_dots = nullptr;
   double *h_alpha = nullptr;  // pinned
   TrialOut *h_out = nullptr;  // pinned
   cudaGraphExec_t trial[2] = {nullptr, nullptr};
   bool own_x0 = false;
+  bool want_xx = true;   // compute x_t . x_t in every trial (needed by a progress callback)
   int eval_kernels = 0;  // kernels of one evaluation inside the trial graph
 };
 
 int free_state(CgState &st) {
   for (int i = 0; i < 2; ++i) {
     if (st.trial[i]) cudaGraphExecDestroy(st.trial[i]);
-    if (i == 1 || st.own_x0) cudaFree(st.xb[i]);
-    cudaFree(st.gb[i]);
+    if ((i == 1 || st.own_x0) && st.xb[i]) cudaFreeAsync(st.xb[i], st.c->stream);
+    if (st.gb[i]) cudaFreeAsync(st.gb[i], st.c->stream);
   }
-  cudaFree(st.s);
-  cudaFree(st.d_alpha);
-  cudaFree(st.d_beta);
-  cudaFree(st.d_part);
-  cudaFree(st.d_dots);
-  if (st.h_alpha) cudaFreeHost(st.h_alpha);
-  if (st.h_out) cudaFreeHost(st.h_out);
+  // stream-ordered frees and pooled pinned slots: nothing here waits for the
+  // other streams of the device
+  for (void *p : {(void *)st.s, (void *)st.d_alpha, (void *)st.d_part, (void *)st.d_dots})
+    if (p) cudaFreeAsync(p, st.c->stream);
+  pinned_small_free(st.h_alpha);
+  pinned_small_free(st.h_out);
   return CCM_OK;
 }
 
@@ -180,13 +182,15 @@ cudaError_t enqueue_trial_tail(CgState &st, const float *xt, const float *gt, co
   cudaStream_t s = st.c->stream;
   cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(gt, st.s, gold, st.n, st.d_part);
   cg_dots_final_kernel<<<1, 1024, 0, s>>>(st.d_part, kDotBlocks, st.d_dots);
-  cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(xt, xt, nullptr, st.n, st.d_part);
-  cg_dots_final_kernel<<<1, 1024, 0, s>>>(st.d_part, kDotBlocks, st.d_dots + 3);
+  if (st.want_xx) {  // ||x_t|| is reported to the progress callback only
+    cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(xt, xt, nullptr, st.n, st.d_part);
+    cg_dots_final_kernel<<<1, 1024, 0, s>>>(st.d_part, kDotBlocks, st.d_dots + 3);
+  }
   cudaError_t e = cudaMemcpyAsync(&st.h_out->f, &st.c->d_out->fx, sizeof(double),
                                   cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(&st.h_out->gs, st.d_dots, 3 * sizeof(double), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && st.want_xx)
     e = cudaMemcpyAsync(&st.h_out->xx, st.d_dots + 4, sizeof(double), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(&st.h_out->status, &st.c->d_out->status, sizeof(int),
@@ -251,19 +255,21 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
   st.c = c;
   st.n = n;
   st.xb[0] = d_x;
+  st.want_xx = progress != nullptr;
   const size_t bytes = sizeof(float) * (size_t)n;
   cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
-  chk(cudaMalloc(&st.xb[1], bytes));
-  chk(cudaMalloc(&st.gb[0], bytes));
-  chk(cudaMalloc(&st.gb[1], bytes));
-  chk(cudaMalloc(&st.s, bytes));
-  chk(cudaMalloc(&st.d_alpha, sizeof(double)));
-  chk(cudaMalloc(&st.d_beta, sizeof(double)));
-  chk(cudaMalloc(&st.d_part, sizeof(double) * 3 * kDotBlocks));
-  chk(cudaMalloc(&st.d_dots, sizeof(double) * 6));
-  chk(cudaMallocHost(&st.h_alpha, sizeof(double)));
-  chk(cudaMallocHost(&st.h_out, sizeof(TrialOut)));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&st.xb[1]), bytes));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&st.gb[0]), bytes));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&st.gb[1]), bytes));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&st.s), bytes));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&st.d_alpha), sizeof(double)));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&st.d_part), sizeof(double) * 3 * kDotBlocks));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&st.d_dots), sizeof(double) * 6));
+  static_assert(sizeof(TrialOut) <= 256, "TrialOut must fit a pinned slot");
+  st.h_alpha = static_cast<double *>(pinned_small_alloc(sizeof(double)));
+  st.h_out = static_cast<TrialOut *>(pinned_small_alloc(sizeof(TrialOut)));
+  if (!st.h_alpha || !st.h_out) chk(cudaErrorMemoryAllocation);
   if (e != cudaSuccess) {
     free_state(st);
     return set_last_error(e == cudaErrorMemoryAllocation ? CCM_ERR_NOMEM : CCM_ERR_CUDA,
@@ -296,8 +302,7 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
     return CCM_OK;
   }
   // s0 = -g0
-  cudaMemsetAsync(st.d_beta, 0, sizeof(double), s);
-  cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[0], st.d_beta, st.s, n);
+  cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[0], 0.0, st.s, n);
   double gs = -gg;  // g.s with s = -g
   double alpha = 1.0 / std::sqrt(gg);
   bool steepest = true;  // s == -g
@@ -313,7 +318,8 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
         }
         *st.h_alpha = alpha;
         e = cudaGraphLaunch(st.trial[p], s);
-        c->launches += st.eval_kernels + 5;  // step + 2 x (dots + final) + evaluation
+        // step + (1 or 2) x (dots + final) + evaluation
+        c->launches += st.eval_kernels + (st.want_xx ? 5 : 3);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) {
           free_state(st);
@@ -338,8 +344,7 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
       }
       if (!accepted && !steepest) {
         // restart along the steepest-descent direction
-        cudaMemsetAsync(st.d_beta, 0, sizeof(double), s);
-        cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[p], st.d_beta, st.s, n);
+        cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[p], 0.0, st.s, n);
         c->launches += 1;
         gs = -gg;
         alpha = 1.0 / std::sqrt(gg);
@@ -359,16 +364,13 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
     double beta = (ggnew - gtg) / gg;
     if (!(beta > 0.0)) beta = 0.0;
     steepest = beta == 0.0;
-    *st.h_alpha = beta;
-    cudaMemcpyAsync(st.d_beta, st.h_alpha, sizeof(double), cudaMemcpyHostToDevice, s);
-    cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[p], st.d_beta, st.s, n);
+    cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[p], beta, st.s, n);
     c->launches += 1;
     // g.s for the new direction: -||g||^2 + beta * (g_t.s_old)
     double gs_new = -ggnew + beta * st.h_out->gs;
     if (!(gs_new < 0.0)) {
       // not a descent direction: restart with steepest descent
-      cudaMemsetAsync(st.d_beta, 0, sizeof(double), s);
-      cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[p], st.d_beta, st.s, n);
+      cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[p], 0.0, st.s, n);
       gs_new = -ggnew;
       steepest = true;
     }
@@ -411,7 +413,7 @@ extern "C" int ccm_conjugrad_host(ccm_context *c, float *x, long long n, const c
   cudaSetDevice(c->device);
   float *d_x = nullptr;
   const size_t bytes = sizeof(float) * (size_t)n;
-  cudaError_t e = cudaMalloc(&d_x, bytes);
+  cudaError_t e = dev_alloc_raw(c, reinterpret_cast<void **>(&d_x), bytes);
   if (e != cudaSuccess)
     return set_last_error(CCM_ERR_NOMEM, "ccm_conjugrad_host: %s", cudaGetErrorString(e));
   e = cudaMemcpyAsync(d_x, x, bytes, cudaMemcpyHostToDevice, c->stream);
@@ -419,7 +421,7 @@ extern "C" int ccm_conjugrad_host(ccm_context *c, float *x, long long n, const c
   if (e == cudaSuccess) rc = ccm_conjugrad_gpu(c, d_x, n, params, progress, instance, result);
   if (e == cudaSuccess && rc == CCM_OK) e = cudaMemcpyAsync(x, d_x, bytes, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  cudaFree(d_x);
+  cudaFreeAsync(d_x, c->stream);
   if (rc != CCM_OK) return rc;
   if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "ccm_conjugrad_host: %s", cudaGetErrorString(e));
   return CCM_OK;

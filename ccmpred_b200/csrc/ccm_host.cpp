@@ -40,6 +40,10 @@ unsigned char aa_to_index(unsigned char c) {
 
 }  // namespace
 
+namespace ccm {
+void init_single_fields(const unsigned char *msa, int ncol, int nrow, float *x);
+}
+
 extern "C" {
 
 // src/ccmpred.c:90-131: V(j,a) = log f_a - log f_gap from pseudocounted column
@@ -47,6 +51,16 @@ extern "C" {
 CCM_API void ccm_init_bias(const unsigned char *msa, int ncol, int nrow, float *x) {
   const long long nvar = ccm_nvar_padded(ncol);
   std::memset(x, 0, sizeof(float) * (size_t)nvar);
+  ccm::init_single_fields(msa, ncol, nrow, x);
+}
+
+}  // extern "C"
+
+namespace ccm {
+
+// The single fields V of init_bias (src/ccmpred.c:101-129): x[a*L + j] for the
+// 20 non-gap states; the rest of x is left as it is.
+void init_single_fields(const unsigned char *msa, int ncol, int nrow, float *x) {
   for (int j = 0; j < ncol; ++j) {
     int counts[kQ];
     for (int a = 0; a < kQ; ++a) counts[a] = 1;
@@ -58,6 +72,10 @@ CCM_API void ccm_init_bias(const unsigned char *msa, int ncol, int nrow, float *
     for (int a = 0; a < kQ - 1; ++a) x[(long long)a * ncol + j] = logf(frac[a]) - gap_log;
   }
 }
+
+}  // namespace ccm
+
+extern "C" {
 
 // src/util.c:16-64: Frobenius norm of the mean-centred 20x20 block of every
 // column pair, zero diagonal.  Returns sqrt(sum of W^2 over k < j, 21x21).

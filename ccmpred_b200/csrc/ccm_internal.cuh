@@ -70,6 +70,18 @@ struct FinalizeArgs {
 // event before the first kernel of an evaluation and one after each kernel.
 constexpr int kMaxProfMarks = 8;
 void prof_mark(ccm_context *c);
+// Stream-ordered device allocation on the context's stream, from its pool.
+cudaError_t dev_alloc_raw(ccm_context *c, void **p, size_t bytes);
+// ccm_create with the pool that the context's device memory comes from.
+int create_context(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
+                   const float *weights, const ccm_options *opt, cudaMemPool_t pool);
+// init_bias restricted to the single fields x[0 .. 20L) (host).
+void init_single_fields(const unsigned char *msa, int ncol, int nrow, float *x);
+// sum_submatrices of a device x into a device L x L map.
+cudaError_t launch_contact_scores(const float *d_x, float *d_out, int L, cudaStream_t stream);
+// Pinned host slots of at most 256 bytes, never returned to CUDA (no device sync).
+void *pinned_small_alloc(size_t bytes);
+void pinned_small_free(void *p);
 void count_launch(ccm_context *c, int n = 1);
 
 cudaError_t tc_configure_kernels();
@@ -100,6 +112,7 @@ struct ccm_context {
   int fwd_pairs = 74;             // resident CTA pairs of tc_forward
   int bwd_pairs = 74;             // resident CTA pairs of tc_backward
   cudaStream_t stream = nullptr;
+  cudaMemPool_t pool = nullptr;   // device memory pool, or null for the device's default pool
   bool own_stream = false;
   int path = CCM_PATH_TC_BF16X2;
   int nsplit = 2;

@@ -77,7 +77,10 @@ typedef struct ccm_options {
 	void *stream;        /* cudaStream_t to run on, or NULL for a private stream that is
 	                        ordered with the legacy default stream */
 	int gradient;        /* CCM_GRADIENT_*; default CCM_GRADIENT_TIED */
-	int pad;
+	int max_sms;         /* upper bound on the SMs the tensor-core kernels of this context
+	                        occupy (rounded down to CTA pairs); 0 = the whole GPU.  Contexts
+	                        that run side by side on one GPU (the batch solver) each take a
+	                        share, so that their persistent kernels stay resident together. */
 } ccm_options;
 
 /* Result of the last evaluation, as kept on the device. */
@@ -274,7 +277,9 @@ typedef struct ccm_batch_params {
 	int workers;                 /* concurrent solves (threads / streams), default 8 */
 	int device;
 	int use_apc;                 /* contact maps with APC (1) or raw Frobenius norms (0) */
-	int pad;
+	int sms_per_worker;          /* max_sms of every worker's contexts; 0 = no limit
+	                                (default; on B200 the 256-alignment batch ran
+	                                fastest with no limit) */
 	ccm_cg_params cg;            /* optimizer settings for every alignment */
 } ccm_batch_params;
 
@@ -308,6 +313,11 @@ CCM_API void ccm_init_bias(const unsigned char *msa, int ncol, int nrow, float *
 /* src/util.c:16-64 sum_submatrices (L x L map); returns the coupling norm the
  * reference prints as "xnorm". */
 CCM_API double ccm_sum_submatrices(const float *x, float *out, int ncol);
+/* The same L x L map (without the xnorm) from a DEVICE x into a DEVICE out,
+ * enqueued on `stream` (a cudaStream_t, NULL for the legacy default stream);
+ * equal to ccm_sum_submatrices bit for bit.  For callers that keep x on the
+ * GPU after ccm_conjugrad_gpu: only L*L floats need to come back to the host. */
+CCM_API int ccm_sum_submatrices_gpu(const float *d_x, float *d_out, int ncol, void *stream);
 /* src/util.c:66-108 apc, in place. */
 CCM_API void ccm_apc(float *mat, int ncol);
 /* src/util.c:110-140 normalize, in place; CCM_ERR_INVALID on a constant map. */

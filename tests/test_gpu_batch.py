@@ -1,6 +1,7 @@
 """Batched solves (ccm_solve_batch): every alignment's result equals that of a
 standalone solve of the same alignment (contexts are independent and each
-solve is deterministic), whatever the number of concurrent workers."""
+solve is deterministic), whatever the number of concurrent workers and the
+share of SMs each worker's contexts may use."""
 import numpy as np
 import pytest
 
@@ -19,6 +20,70 @@ def test_batch_matches_standalone_solves(gpu):
         assert r4.iterations == r1.iterations and r4.fx == r1.fx
         assert np.array_equal(m4, m1)
         assert np.all(np.isfinite(m4))
+
+
+@pytest.mark.parametrize("gradient", ["tied", "partial"])
+def test_sm_share_gives_identical_results(gpu, gradient):
+    """max_sms only changes which CTA pair runs which tile: every tile is computed
+    the same way, the loss partials are summed in a fixed order and every gradient
+    element receives exactly one add, so f and g are bit-for-bit the same."""
+    import torch
+    from ccmpred_b200 import Evaluator
+    msa = synth.generate(synth.MSAConfig("share", 150, 1400, n_pairs=10, seed=71))
+    x = torch.from_numpy(synth.random_x(150, 72, symmetric=(gradient == "tied"))).cuda()
+    out = []
+    for max_sms in (0, 30, 8, 2):
+        ev = Evaluator(msa, gradient=gradient, max_sms=max_sms)
+        g = torch.empty_like(x)
+        f = ev.evaluate(x, g)
+        out.append((f, g.cpu().numpy()))
+        ev.close()
+    for f, g in out[1:]:
+        assert f == out[0][0]
+        assert np.array_equal(g, out[0][1])
+
+
+def test_batch_with_explicit_share(gpu):
+    msas = [m[:800] for m in synth.batch_workload(4, seed0=600)]
+    ra, ma = solve_batch(msas, workers=2, max_iterations=15, sms_per_worker=12)
+    rb, mb = solve_batch(msas, workers=2, max_iterations=15, sms_per_worker=-1)
+    for a, b, x, y in zip(ra, rb, ma, mb):
+        assert a.iterations == b.iterations and a.fx == b.fx
+        assert np.array_equal(x, y)
+
+
+def test_device_contact_scores_match_host(gpu):
+    """ccm_sum_submatrices_gpu reproduces the host sum_submatrices (the reference's
+    order of float operations) bit for bit."""
+    import torch
+    from ccmpred_b200 import host
+    from ccmpred_b200._lib import lib
+    for L, seed in ((7, 1), (37, 2), (130, 3)):
+        x = synth.random_x(L, seed, v_sd=0.3, w_sd=0.2, symmetric=(seed != 2))
+        want, _ = host.contact_map(x, L, apc=False)
+        xd = torch.from_numpy(x).cuda()
+        out = torch.empty(L * L, dtype=torch.float32, device="cuda")
+        assert lib().ccm_sum_submatrices_gpu(xd.data_ptr(), out.data_ptr(), L, None) == 0
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy().reshape(L, L), want)
+
+
+def test_batch_map_equals_standalone_pipeline(gpu):
+    """The batch keeps x on the device and computes the contact map there; the map
+    equals that of the host pipeline: weights, init_bias, the device CG, then the
+    host sum_submatrices and APC."""
+    import torch
+    from ccmpred_b200 import Evaluator, calculate_weights, host
+    msa = synth.generate(synth.MSAConfig("pipe", 90, 700, n_pairs=9, seed=77))
+    res, maps = solve_batch([msa], workers=1, max_iterations=25, epsilon=1e-3)
+    w = calculate_weights(msa, 0.8)
+    ev = Evaluator(msa, weights=w)
+    x = torch.from_numpy(host.init_bias(msa)).cuda()
+    r = ev.minimize(x, max_iterations=25, epsilon=1e-3)
+    ev.close()
+    want, _ = host.contact_map(x.cpu().numpy(), 90, apc=True)
+    assert res[0].iterations == r.iterations and res[0].fx == r.fx
+    assert np.array_equal(maps[0], want)
 
 
 def test_batch_rejects_bad_input(gpu):
