@@ -296,6 +296,22 @@ void free_prof(ccm_context *c) {
 
 }  // namespace
 
+int ccm::enqueue_evaluation_step(ccm_context *c, const float *d_x, const float *d_s,
+                                  const double *d_alpha, float *d_xt, float *d_g) {
+  if (c->path != CCM_PATH_TC_BF16X2 && c->path != CCM_PATH_TC_BF16X3)
+    return set_error(CCM_ERR_INVALID, "fused step: tensor-core paths only");
+  CCM_CUDA_TRY(cudaMemsetAsync(c->d_out, 0, sizeof(ccm_result), c->stream));
+  c->prof_idx = 0;
+  const cudaError_t e = tc_evaluate_step(c, d_x, d_s, d_alpha, d_xt, d_g);
+  if (e != cudaSuccess)
+    return set_error(CCM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+  if (c->prof_on && c->prof_eval < c->prof_max) {
+    c->prof_marks_used = c->prof_idx;
+    c->prof_eval++;
+  }
+  return CCM_OK;
+}
+
 int ccm::enqueue_evaluation(ccm_context *c, const float *d_x, float *d_g) {
   return enqueue_eval(c, d_x, d_g);
 }

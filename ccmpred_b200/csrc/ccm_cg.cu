@@ -24,7 +24,9 @@
 // tests are FP64.  One trial step (x_t = x + alpha s, the four evaluation
 // kernels, the dots, the copy of the scalars to pinned host memory) is
 // captured once in a CUDA graph per buffer parity and replayed; the host only
-// reads back 40 bytes per trial.
+// reads back 40 bytes per trial.  On the tensor-core paths the step is fused
+// into tc_prep, which reads x and s once and writes x_t while it splits the
+// couplings into their bf16 terms.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -38,6 +40,8 @@ namespace ccm {
 
 int set_last_error(int code, const char *fmt, ...);
 int enqueue_evaluation(ccm_context *c, const float *d_x, float *d_g);
+int enqueue_evaluation_step(ccm_context *c, const float *d_x, const float *d_s,
+                            const double *d_alpha, float *d_xt, float *d_g);
 
 constexpr int kDotBlocks = 592;  // 4 x 148 SMs
 
@@ -153,7 +157,7 @@ struct CgState {
   cudaGraphExec_t trial[2] = {nullptr, nullptr};
   bool own_x0 = false;
   bool want_xx = true;   // compute x_t . x_t in every trial (needed by a progress callback)
-  int eval_kernels = 0;  // kernels of one evaluation inside the trial graph
+  int eval_kernels = 0;  // kernels of the step and the evaluation inside the trial graph
 };
 
 int free_state(CgState &st) {
@@ -208,10 +212,14 @@ int capture_trial(CgState &st, int p) {
   cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "cg capture: %s", cudaGetErrorString(e));
   cudaMemcpyAsync(st.d_alpha, st.h_alpha, sizeof(double), cudaMemcpyHostToDevice, s);
-  cg_step_kernel<<<grid_for(st.n), 256, 0, s>>>(x, st.s, st.d_alpha, xt, st.n);
+  // tensor-core paths take the step inside tc_prep (one pass over x and s that
+  // also splits the couplings into the bf16 terms); the CUDA-core paths step first
+  const bool fused = st.c->path == CCM_PATH_TC_BF16X2 || st.c->path == CCM_PATH_TC_BF16X3;
+  if (!fused) cg_step_kernel<<<grid_for(st.n), 256, 0, s>>>(x, st.s, st.d_alpha, xt, st.n);
   const long long before = st.c->launches;
-  int rc = enqueue_evaluation(st.c, xt, gt);
-  st.eval_kernels = (int)(st.c->launches - before);
+  int rc = fused ? enqueue_evaluation_step(st.c, x, st.s, st.d_alpha, xt, gt)
+                 : enqueue_evaluation(st.c, xt, gt);
+  st.eval_kernels = (int)(st.c->launches - before) + (fused ? 0 : 1);
   st.c->launches = before;  // counted per replay instead
   e = enqueue_trial_tail(st, xt, gt, g);
   cudaError_t e2 = cudaStreamEndCapture(s, &graph);
@@ -318,8 +326,8 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
         }
         *st.h_alpha = alpha;
         e = cudaGraphLaunch(st.trial[p], s);
-        // step + (1 or 2) x (dots + final) + evaluation
-        c->launches += st.eval_kernels + (st.want_xx ? 5 : 3);
+        // (step +) evaluation + (1 or 2) x (dots + final)
+        c->launches += st.eval_kernels + (st.want_xx ? 4 : 2);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) {
           free_state(st);

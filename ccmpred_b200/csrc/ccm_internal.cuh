@@ -26,6 +26,12 @@ struct BwdMaps {
 
 struct PrepArgs {
   __nv_bfloat16 *wperm[3];
+  // Fused CG step (tc_prep<.., true>): the parameters evaluated are
+  // xt = x + alpha * s, computed here, written to xt and used at once.
+  const float *step_x, *step_s;  // full vectors (nvar_padded)
+  const double *alpha;           // device scalar
+  float *xt;                     // full vector out
+  long long nsp;                 // nsingle_padded
   double *part_reg;
   int L, S;
   float lambda_pair;
@@ -89,6 +95,10 @@ cudaError_t tc_configure_kernels();
 cudaError_t tc_forward_max_pairs(int nsplit, int *pairs);
 cudaError_t tc_backward_max_pairs(int nsplit, int *pairs);
 cudaError_t tc_evaluate(ccm_context *c, const float *d_x, float *d_g);
+// One CG trial on a tensor-core context: xt = x + alpha s (alpha on the device),
+// then the evaluation at xt, with the step fused into tc_prep.
+cudaError_t tc_evaluate_step(ccm_context *c, const float *d_x, const float *d_s,
+                             const double *d_alpha, float *d_xt, float *d_g);
 int tc_fwd_smem_bytes(int nsplit);
 int tc_bwd_smem_bytes(int nsplit);
 
@@ -100,6 +110,10 @@ int set_last_error(int code, const char *fmt, ...);
 
 // Enqueue one evaluation of the context's path on its stream (no host sync).
 int enqueue_evaluation(ccm_context *c, const float *d_x, float *d_g);
+// Tensor-core paths: d_xt = d_x + alpha d_s (alpha on the device) fused into the
+// evaluation at d_xt.
+int enqueue_evaluation_step(ccm_context *c, const float *d_x, const float *d_s,
+                            const double *d_alpha, float *d_xt, float *d_g);
 
 cudaError_t reweight_counts(const uint8_t *d_msa, int L, int N, int idthres, int *d_counts,
                             cudaStream_t stream);

@@ -30,12 +30,30 @@ namespace ccm {
 // regulariser gradient 2*lambda2*x (src/evaluate_cpu.c:158-161); tc_backward
 // later adds the data term with one atomic add per element.  One FP64 partial
 // of sum x^2 per row (all 32 L slots).
-template <int NSPLIT>
+//
+// STEP = true fuses the conjugate-gradient trial step into this pass: each
+// element is v = fmaf(alpha, s, x) of the current iterate x and direction s
+// (the same operation as the stand-alone step kernel), written to xt and used
+// for everything above; one extra block (the last) steps the single fields.
+template <int NSPLIT, bool STEP>
 __global__ void __launch_bounds__(256) tc_prep_kernel(const float *__restrict__ x2,
                                                       float *__restrict__ g2, PrepArgs args) {
   extern __shared__ __align__(16) float xrow[];  // 21 L floats
   const int L = args.L;
   const int row = blockIdx.x;  // b*L + k
+  float a = 0.0f;
+  const float *s2 = nullptr;
+  float *xt2 = nullptr;
+  if (STEP) {
+    a = (float)args.alpha[0];
+    if (row == kQ * L) {
+      for (long long i = threadIdx.x; i < args.nsp; i += blockDim.x)
+        args.xt[i] = fmaf(a, args.step_s[i], args.step_x[i]);
+      return;
+    }
+    s2 = args.step_s + args.nsp;
+    xt2 = args.xt + args.nsp;
+  }
   const int b = row / L, k = row % L;
   const long long base = (long long)row * kQPad * L;
   const float two_l2 = args.g2_coef * args.lambda_pair;  // 2 (tied) or 1 (partial)
@@ -55,6 +73,12 @@ __global__ void __launch_bounds__(256) tc_prep_kernel(const float *__restrict__ 
       for (int u = 0; u < kU; ++u) {
         const int i = i0 + u * blockDim.x;
         v[u] = i < n4 ? __ldcs(src + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (STEP && i < n4) {
+          const float4 sv = __ldcs(reinterpret_cast<const float4 *>(s2 + base) + i);
+          v[u] = make_float4(fmaf(a, sv.x, v[u].x), fmaf(a, sv.y, v[u].y), fmaf(a, sv.z, v[u].z),
+                             fmaf(a, sv.w, v[u].w));
+          reinterpret_cast<float4 *>(xt2 + base)[i] = v[u];
+        }
       }
 #pragma unroll
       for (int u = 0; u < kU; ++u) {
@@ -70,13 +94,15 @@ __global__ void __launch_bounds__(256) tc_prep_kernel(const float *__restrict__ 
     }
   } else {
     for (int i = threadIdx.x; i < nreal; i += blockDim.x) {
-      const float v = x2[base + i];
+      float v = x2[base + i];
+      if (STEP) { v = fmaf(a, s2[base + i], v); xt2[base + i] = v; }
       acc += (double)v * v;
       xrow[i] = v;
       g2[base + i] = two_l2 * v;
     }
     for (int i = nreal + threadIdx.x; i < kQPad * L; i += blockDim.x) {
-      const float v = x2[base + i];
+      float v = x2[base + i];
+      if (STEP) { v = fmaf(a, s2[base + i], v); xt2[base + i] = v; }
       acc += (double)v * v;
       g2[base + i] = two_l2 * v;
     }
@@ -825,19 +851,31 @@ __global__ void __launch_bounds__(1024) tc_finalize_kernel(FinalizeArgs args) {
 }
 
 // ---------------------------------------------------------------- launchers
+// Without a step: evaluate at d_x.  With one (step_x, step_s, alpha): evaluate
+// at d_x := step_x + alpha * step_s, which tc_prep computes and writes to d_x.
 template <int NSPLIT>
-static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g) {
+static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g,
+                             const float *step_x = nullptr, const float *step_s = nullptr,
+                             const double *alpha = nullptr) {
   const int L = c->L;
   const float *x1 = d_x;
   const float *x2 = d_x + c->nsp;
   float *g2 = d_g + c->nsp;
+  const bool step = step_x != nullptr;
 
   PrepArgs pa{};
   pa.L = L; pa.S = c->S; pa.lambda_pair = c->lambda_pair; pa.part_reg = c->d_part_reg;
   pa.g2_coef = c->gradient == CCM_GRADIENT_PARTIAL ? 1.0f : 2.0f;
   for (int i = 0; i < 3; ++i) pa.wperm[i] = c->d_wperm[i];
   prof_mark(c);
-  tc_prep_kernel<NSPLIT><<<kQ * L, 256, sizeof(float) * kQ * L, c->stream>>>(x2, g2, pa);
+  if (step) {
+    pa.step_x = step_x; pa.step_s = step_s; pa.alpha = alpha;
+    pa.xt = const_cast<float *>(d_x); pa.nsp = c->nsp;
+    tc_prep_kernel<NSPLIT, true><<<kQ * L + 1, 256, sizeof(float) * kQ * L, c->stream>>>(
+        step_x + c->nsp, g2, pa);
+  } else {
+    tc_prep_kernel<NSPLIT, false><<<kQ * L, 256, sizeof(float) * kQ * L, c->stream>>>(x2, g2, pa);
+  }
   prof_mark(c);
 
   FwdArgs fa{};
@@ -905,9 +943,13 @@ cudaError_t tc_forward_max_pairs(int nsplit, int *pairs) {
 cudaError_t tc_configure_kernels() {
   cudaError_t e;
   // the staged W row is 21 L floats: up to L = 2000 (168 KB)
-  e = cudaFuncSetAttribute(tc_prep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 168000);
+  e = cudaFuncSetAttribute(tc_prep_kernel<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 168000);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(tc_prep_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 168000);
+  e = cudaFuncSetAttribute(tc_prep_kernel<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 168000);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(tc_prep_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 168000);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(tc_prep_kernel<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 168000);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(tc_forward_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            FwdSmem<2>::kTotal);
@@ -930,6 +972,12 @@ cudaError_t tc_configure_kernels() {
 
 cudaError_t tc_evaluate(ccm_context *c, const float *d_x, float *d_g) {
   return c->nsplit == 3 ? launch_tc<3>(c, d_x, d_g) : launch_tc<2>(c, d_x, d_g);
+}
+
+cudaError_t tc_evaluate_step(ccm_context *c, const float *d_x, const float *d_s,
+                             const double *d_alpha, float *d_xt, float *d_g) {
+  return c->nsplit == 3 ? launch_tc<3>(c, d_xt, d_g, d_x, d_s, d_alpha)
+                        : launch_tc<2>(c, d_xt, d_g, d_x, d_s, d_alpha);
 }
 
 int tc_fwd_smem_bytes(int nsplit) { return nsplit == 3 ? FwdSmem<3>::kTotal : FwdSmem<2>::kTotal; }

@@ -73,3 +73,22 @@ def planted_pairs(cfg):
     npairs = min(cfg.n_pairs, L // 2)
     cols = rng.permutation(L)[: 2 * npairs].reshape(npairs, 2)
     return {(int(min(a, b)), int(max(a, b))) for a, b in cols}
+
+
+@pytest.mark.parametrize("path", ["tc_bf16x2", "tc_bf16x3", "simt_f32"])
+def test_cg_result_is_the_evaluation_at_the_returned_x(gpu, path):
+    """On the tensor-core paths each trial's step x_t = x + alpha s is fused into
+    tc_prep, which writes x_t and evaluates it in the same pass.  The x that the
+    CG returns is such an x_t: evaluating it again must give the CG's f exactly,
+    and the gradient left in the CG's last accepted trial is that of this x."""
+    import torch
+    msa = synth.generate(synth.MSAConfig("cgstep", 53, 700, n_pairs=5, seed=63))
+    ev = Evaluator(msa, path=path)
+    for iters in (1, 7):
+        xd = torch.from_numpy(init_bias(msa)).cuda()
+        res = ev.minimize(xd, max_iterations=iters, epsilon=0.0)
+        g = torch.empty_like(xd)
+        f = ev.evaluate(xd, g)
+        assert f == res.fx
+        assert abs(float(torch.linalg.vector_norm(g.double())) - res.gnorm) <= 1e-12 * res.gnorm
+    ev.close()
