@@ -44,13 +44,25 @@ UNIT = "evals/s"
 WORKLOAD = "L300_N5000"
 
 
+
+PATH_DTYPE = {"tc_bf16x2": "bf16", "tc_bf16x3": "bf16", "tc_i8x3": "int8"}
+PATH_ARITHMETIC = {
+    "tc_bf16x2": "bf16 hi+lo split operands, f32 tensor-core accumulation, "
+                 "f64 loss/regulariser reductions",
+    "tc_bf16x3": "three bf16 terms per operand, f32 tensor-core accumulation, "
+                 "f64 loss/regulariser reductions",
+    "tc_i8x3": "W and R as three 8-bit fixed-point digits (21 fractional bits, per-column "
+               "power-of-two scale for W), exact s32 tensor-core accumulation, "
+               "f64 loss/regulariser reductions",
+}
+
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--path", default="tc_bf16x2", choices=["tc_bf16x2", "tc_bf16x3"])
+    p.add_argument("--path", default="tc_bf16x2", choices=["tc_bf16x2", "tc_bf16x3", "tc_i8x3"])
     p.add_argument("--e2e-steps", type=int, default=50)
     p.add_argument("--plain-steps", type=int, default=20)
     p.add_argument("--cpu-budget-s", type=float, default=15.0)
@@ -426,7 +438,9 @@ def main():
         # tensor-core flops actually issued by the dominant kernel: every split term,
         # the padded shapes (S = 256 slots per 12 columns, rows padded to 256) and,
         # for the backward, both products O^T R and R^T O on the upper-triangle tiles
-        nsplit = 3 if args.path == "tc_bf16x3" else 2
+        # bf16-equivalent products per element: 2 (hi+lo), 3 (three terms); the integer
+        # path does three 8-bit products at twice the bf16 rate = 1.5
+        nsplit = {"tc_bf16x3": 3, "tc_i8x3": 1.5}.get(args.path, 2)
         T = (L + 11) // 12
         S, Npad = 256 * T, (N + 255) // 256 * 256
         executed = {"tc_forward": 2.0 * Npad * S * S * nsplit,
@@ -470,12 +484,12 @@ def main():
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": PATH_DTYPE[args.path],
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "ncol": L, "nrow": N, "planted_pairs": cfg.n_pairs,
                        "seed": cfg.seed, "path": args.path,
-                       "arithmetic": "bf16 hi+lo split operands, f32 tensor-core accumulation, "
-                                     "f64 loss/regulariser reductions",
+                       "arithmetic": PATH_ARITHMETIC[args.path],
                        "l2": "inputs larger than L2 (x and g 242 MB each, bf16 W terms 164 MB)",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "tensor", "kernel": dom, "achieved": achieved, "peak": peak,

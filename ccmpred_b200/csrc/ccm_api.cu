@@ -141,6 +141,25 @@ int make_map_bf16(CUtensorMap *map, void *base, long long rows, long long cols, 
   return CCM_OK;
 }
 
+// 2-D 8-bit row-major [rows][cols] tensor, boxes of box_cols x box_rows bytes
+// (128-byte swizzle for 128-column boxes, 64-byte swizzle for 64-column boxes).
+int make_map_u8(CUtensorMap *map, void *base, long long rows, long long cols, int box_cols,
+                int box_rows) {
+  const CUtensorMapSwizzle swz =
+      box_cols == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
+  EncodeTiledFn enc = get_encode_fn();
+  if (!enc) return set_error(CCM_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)cols};
+  cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(CCM_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return CCM_OK;
+}
+
 // One-hot matrix O[n][s] (bf16): 1 where the state of column l(s) in row n is
 // q(s); 1 in the ones slot for every real row; 0 elsewhere (padding rows,
 // padding slots).
@@ -178,6 +197,7 @@ int ensure_configured(int device) {
   std::lock_guard<std::mutex> lock(configure_mutex);
   if (configured[device]) return CCM_OK;
   CCM_CUDA_TRY(tc_configure_kernels());
+  CCM_CUDA_TRY(i8_configure_kernels());
   CCM_CUDA_TRY(simt_configure_kernels());
   configured[device] = true;
   return CCM_OK;
@@ -189,12 +209,26 @@ int alloc_tc(ccm_context *c) {
   // rows padded to the forward's 256-row CTA-pair tiles
   c->Npad = ((c->N + 255) / 256) * 256;
   const size_t S = c->S, Np = c->Npad;
-  CCM_CUDA_TRY(dev_alloc(c, &c->d_onehot, sizeof(__nv_bfloat16) * Np * S));
-  for (int i = 0; i < c->nsplit; ++i) {
-    CCM_CUDA_TRY(dev_alloc(c, &c->d_wperm[i], sizeof(__nv_bfloat16) * S * S));
-    CCM_CUDA_TRY(cudaMemsetAsync(c->d_wperm[i], 0, sizeof(__nv_bfloat16) * S * S, c->stream));
-    CCM_CUDA_TRY(dev_alloc(c, &c->d_r[i], sizeof(__nv_bfloat16) * Np * S));
-    CCM_CUDA_TRY(cudaMemsetAsync(c->d_r[i], 0, sizeof(__nv_bfloat16) * Np * S, c->stream));
+  const bool i8 = c->path == CCM_PATH_TC_I8X3;
+  if (i8) {
+    // integer path: one-hot x1 / x128 bytes, three digit matrices of W and of R
+    CCM_CUDA_TRY(dev_alloc(c, &c->d_o1, Np * S));
+    CCM_CUDA_TRY(dev_alloc(c, &c->d_o128, Np * S));
+    for (int i = 0; i < 3; ++i) {
+      CCM_CUDA_TRY(dev_alloc(c, &c->d_wdig[i], S * S));
+      CCM_CUDA_TRY(cudaMemsetAsync(c->d_wdig[i], 0, S * S, c->stream));
+      CCM_CUDA_TRY(dev_alloc(c, &c->d_rdig[i], Np * S));
+      CCM_CUDA_TRY(cudaMemsetAsync(c->d_rdig[i], 0, Np * S, c->stream));
+    }
+    CCM_CUDA_TRY(dev_alloc(c, &c->d_colmax, sizeof(uint32_t) * kQ * c->L));
+  } else {
+    CCM_CUDA_TRY(dev_alloc(c, &c->d_onehot, sizeof(__nv_bfloat16) * Np * S));
+    for (int i = 0; i < c->nsplit; ++i) {
+      CCM_CUDA_TRY(dev_alloc(c, &c->d_wperm[i], sizeof(__nv_bfloat16) * S * S));
+      CCM_CUDA_TRY(cudaMemsetAsync(c->d_wperm[i], 0, sizeof(__nv_bfloat16) * S * S, c->stream));
+      CCM_CUDA_TRY(dev_alloc(c, &c->d_r[i], sizeof(__nv_bfloat16) * Np * S));
+      CCM_CUDA_TRY(cudaMemsetAsync(c->d_r[i], 0, sizeof(__nv_bfloat16) * Np * S, c->stream));
+    }
   }
   const long long fwd_tiles = (long long)(c->Npad / 128) * c->T;
   CCM_CUDA_TRY(dev_alloc(c, &c->d_part_f, sizeof(double) * fwd_tiles * 8));
@@ -212,6 +246,21 @@ int alloc_tc(ccm_context *c) {
   CCM_CUDA_TRY(cudaMemcpyAsync(c->d_bwd_tiles, tiles.data(), sizeof(int2) * tiles.size(),
                                cudaMemcpyHostToDevice, c->stream));
 
+  int rc;
+  if (i8) {
+    CCM_CUDA_TRY(i8_build_onehot(c));
+    std::memset(&c->i8fwd_maps, 0, sizeof(c->i8fwd_maps));
+    std::memset(&c->i8bwd_maps, 0, sizeof(c->i8bwd_maps));
+    if ((rc = make_map_u8(&c->i8fwd_maps.a1, c->d_o1, Np, S, 64, 128)) != CCM_OK) return rc;
+    if ((rc = make_map_u8(&c->i8fwd_maps.a128, c->d_o128, Np, S, 64, 128)) != CCM_OK) return rc;
+    if ((rc = make_map_u8(&c->i8bwd_maps.o1, c->d_o1, Np, S, 128, 32)) != CCM_OK) return rc;
+    if ((rc = make_map_u8(&c->i8bwd_maps.o128, c->d_o128, Np, S, 128, 32)) != CCM_OK) return rc;
+    for (int i = 0; i < 3; ++i) {
+      if ((rc = make_map_u8(&c->i8fwd_maps.b[i], c->d_wdig[i], S, S, 128, 64)) != CCM_OK) return rc;
+      if ((rc = make_map_u8(&c->i8bwd_maps.r[i], c->d_rdig[i], Np, S, 128, 32)) != CCM_OK) return rc;
+    }
+    return CCM_OK;
+  }
   const long long total = (long long)Np * S;
   build_onehot_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c->stream>>>(
       c->d_msa, c->d_onehot, c->L, c->N, c->S, c->Npad);
@@ -219,7 +268,6 @@ int alloc_tc(ccm_context *c) {
 
   std::memset(&c->fwd_maps, 0, sizeof(c->fwd_maps));
   std::memset(&c->bwd_maps, 0, sizeof(c->bwd_maps));
-  int rc;
   if ((rc = make_map_bf16(&c->fwd_maps.a, c->d_onehot, Np, S, 32, 128)) != CCM_OK) return rc;
   if ((rc = make_map_bf16(&c->bwd_maps.o, c->d_onehot, Np, S, 64, 32)) != CCM_OK) return rc;
   for (int i = 0; i < c->nsplit; ++i) {
@@ -242,7 +290,8 @@ void free_all(ccm_context *c) {
   // stream-ordered frees: cudaFree would wait for every stream of the device
   auto f = [c](void *p) { if (p) cudaFreeAsync(p, c->stream); };
   f(c->d_msa); f(c->d_w); f(c->d_out); f(c->d_onehot);
-  for (int i = 0; i < 3; ++i) { f(c->d_wperm[i]); f(c->d_r[i]); }
+  for (int i = 0; i < 3; ++i) { f(c->d_wperm[i]); f(c->d_r[i]); f(c->d_wdig[i]); f(c->d_rdig[i]); }
+  f(c->d_o1); f(c->d_o128); f(c->d_colmax);
   f(c->d_part_f); f(c->d_part_reg); f(c->d_g1d); f(c->d_bwd_tiles);
   f(c->d_simt_pc); f(c->d_simt_g2); f(c->d_simt_part); f(c->d_simt_g1);
   f(c->d_xh); f(c->d_gh);
@@ -270,6 +319,7 @@ int enqueue_eval(ccm_context *c, const float *d_x, float *d_g) {
   switch (c->path) {
     case CCM_PATH_TC_BF16X2:
     case CCM_PATH_TC_BF16X3: e = tc_evaluate(c, d_x, d_g); break;
+    case CCM_PATH_TC_I8X3: e = i8_evaluate(c, d_x, d_g, nullptr, nullptr, nullptr); break;
     case CCM_PATH_SIMT_F32: e = simt_evaluate(c, d_x, d_g); break;
     case CCM_PATH_SIMT_F64:
       return set_error(CCM_ERR_INVALID, "CCM_PATH_SIMT_F64 takes double buffers: use ccm_evaluate_f64");
@@ -298,11 +348,14 @@ void free_prof(ccm_context *c) {
 
 int ccm::enqueue_evaluation_step(ccm_context *c, const float *d_x, const float *d_s,
                                   const double *d_alpha, float *d_xt, float *d_g) {
-  if (c->path != CCM_PATH_TC_BF16X2 && c->path != CCM_PATH_TC_BF16X3)
+  if (c->path != CCM_PATH_TC_BF16X2 && c->path != CCM_PATH_TC_BF16X3 &&
+      c->path != CCM_PATH_TC_I8X3)
     return set_error(CCM_ERR_INVALID, "fused step: tensor-core paths only");
   CCM_CUDA_TRY(cudaMemsetAsync(c->d_out, 0, sizeof(ccm_result), c->stream));
   c->prof_idx = 0;
-  const cudaError_t e = tc_evaluate_step(c, d_x, d_s, d_alpha, d_xt, d_g);
+  const cudaError_t e = c->path == CCM_PATH_TC_I8X3
+                            ? i8_evaluate(c, d_x, d_g, d_s, d_alpha, d_xt)
+                            : tc_evaluate_step(c, d_x, d_s, d_alpha, d_xt, d_g);
   if (e != cudaSuccess)
     return set_error(CCM_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
   if (c->prof_on && c->prof_eval < c->prof_max) {
@@ -367,7 +420,7 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
   *out = nullptr;
   ccm_options o;
   if (opt) o = *opt; else ccm_options_default(&o, ncol);
-  if (o.path < CCM_PATH_TC_BF16X2 || o.path > CCM_PATH_SIMT_F64)
+  if (o.path < CCM_PATH_TC_BF16X2 || o.path > CCM_PATH_TC_I8X3)
     return set_error(CCM_ERR_INVALID, "ccm_create: unknown path %d", o.path);
   if (o.gradient != CCM_GRADIENT_TIED && o.gradient != CCM_GRADIENT_PARTIAL)
     return set_error(CCM_ERR_INVALID, "ccm_create: unknown gradient mode %d", o.gradient);
@@ -380,7 +433,9 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
   CCM_CUDA_TRY(cudaSetDevice(o.device));
   cudaDeviceProp prop;
   CCM_CUDA_TRY(cudaGetDeviceProperties(&prop, o.device));
-  if ((o.path == CCM_PATH_TC_BF16X2 || o.path == CCM_PATH_TC_BF16X3) && prop.major != 10)
+  const bool tc_path = o.path == CCM_PATH_TC_BF16X2 || o.path == CCM_PATH_TC_BF16X3 ||
+                       o.path == CCM_PATH_TC_I8X3;
+  if (tc_path && prop.major != 10)
     return set_error(CCM_ERR_UNSUPPORTED, "tensor-core path needs an sm_100 device (found sm_%d%d)",
                      prop.major, prop.minor);
   int rc = ensure_configured(o.device);
@@ -390,10 +445,13 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
   c->pool = pool;
   c->device = o.device;
   c->num_sms = prop.multiProcessorCount;
-  if (o.path == CCM_PATH_TC_BF16X2 || o.path == CCM_PATH_TC_BF16X3) {
+  if (tc_path) {
     const int ns = o.path == CCM_PATH_TC_BF16X3 ? 3 : 2;
-    cudaError_t e = tc_forward_max_pairs(ns, &c->fwd_pairs);
-    if (e == cudaSuccess) e = tc_backward_max_pairs(ns, &c->bwd_pairs);
+    cudaError_t e = o.path == CCM_PATH_TC_I8X3 ? i8_forward_max_pairs(&c->fwd_pairs)
+                                               : tc_forward_max_pairs(ns, &c->fwd_pairs);
+    if (e == cudaSuccess)
+      e = o.path == CCM_PATH_TC_I8X3 ? i8_backward_max_pairs(&c->bwd_pairs)
+                                     : tc_backward_max_pairs(ns, &c->bwd_pairs);
     if (e != cudaSuccess || c->fwd_pairs < 1 || c->bwd_pairs < 1) {
       delete c;
       return set_error(CCM_ERR_CUDA, "tc_forward cluster occupancy: %s", cudaGetErrorString(e));
@@ -444,7 +502,7 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
   if (!c->h_out) return fail(set_error(CCM_ERR_NOMEM, "pinned result record"));
   c->d_status = &c->d_out->status;
 
-  if (c->path == CCM_PATH_TC_BF16X2 || c->path == CCM_PATH_TC_BF16X3) {
+  if (tc_path) {
     if ((rc = alloc_tc(c)) != CCM_OK) return fail(rc);
   } else {
     if ((rc = alloc_simt(c, c->path == CCM_PATH_SIMT_F64 ? sizeof(double) : sizeof(float))) != CCM_OK)
@@ -546,7 +604,15 @@ long long ccm_debug_copy(ccm_context *c, int which, void *dst, long long bytes) 
   const void *src = nullptr;
   long long size = 0;
   const long long slots = (long long)c->S;
-  if (which == 0) { src = c->d_onehot; size = 2LL * c->Npad * slots; }
+  if (c->path == CCM_PATH_TC_I8X3) {
+    // integer path: 0 one-hot (x1 bytes), 1-3 digits of W, 4-6 digits of R,
+    // 7 single-field data gradient, 8 column maxima of |W| (float bits)
+    if (which == 0) { src = c->d_o1; size = (long long)c->Npad * slots; }
+    else if (which >= 1 && which <= 3) { src = c->d_wdig[which - 1]; size = slots * slots; }
+    else if (which >= 4 && which <= 6) { src = c->d_rdig[which - 4]; size = (long long)c->Npad * slots; }
+    else if (which == 7) { src = c->d_g1d; size = 4LL * (kQ - 1) * c->L; }
+    else if (which == 8) { src = c->d_colmax; size = 4LL * kQ * c->L; }
+  } else if (which == 0) { src = c->d_onehot; size = 2LL * c->Npad * slots; }
   else if (which >= 1 && which <= 3) { src = c->d_wperm[which - 1]; size = 2LL * slots * slots; }
   else if (which >= 4 && which <= 6) { src = c->d_r[which - 4]; size = 2LL * c->Npad * slots; }
   else if (which == 7) { src = c->d_g1d; size = 4LL * (kQ - 1) * c->L; }

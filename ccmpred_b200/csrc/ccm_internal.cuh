@@ -24,6 +24,37 @@ struct BwdMaps {
   CUtensorMap r[3];   // R_i       [Npad][S], same box
 };
 
+// Integer path (CCM_PATH_TC_I8X3): 8-bit operands, s32 tensor-core accumulation.
+struct I8FwdMaps {
+  CUtensorMap a1, a128;  // one-hot O x1 / x128 [Npad][S] u8, box 64 (slots, K) x 128 (rows), 64B swizzle
+  CUtensorMap b[3];      // digits of W [S][S] s8, box 128 (out slots, N) x 64 (in slots, K), 128B swizzle
+};
+
+struct I8BwdMaps {
+  CUtensorMap o1, o128;  // one-hot O x1 / x128 [Npad][S] u8, box 128 (slots) x 32 (rows), 128B swizzle
+  CUtensorMap r[3];      // digits of R [Npad][S] s8, same box
+};
+
+struct I8PrepArgs {
+  int8_t *wdig[3];
+  const uint32_t *colmax;  // per coupling column (a*L + j): max |W| as float bits
+  double *part_reg;
+  int L, S;
+  float lambda_pair;
+  float g2_coef;
+};
+
+struct I8FwdArgs {
+  const uint8_t *msa;
+  const float *w;
+  const float *x1;
+  const uint32_t *colmax;
+  int8_t *r[3];
+  double *part_f;
+  int *status;
+  int L, N, S, T, Npad, m_tiles;
+};
+
 struct PrepArgs {
   __nv_bfloat16 *wperm[3];
   // Fused CG step (tc_prep<.., true>): the parameters evaluated are
@@ -95,6 +126,15 @@ cudaError_t tc_configure_kernels();
 cudaError_t tc_forward_max_pairs(int nsplit, int *pairs);
 cudaError_t tc_backward_max_pairs(int nsplit, int *pairs);
 cudaError_t tc_evaluate(ccm_context *c, const float *d_x, float *d_g);
+// The integer path: evaluation at d_x, or (d_s != null) at d_xt = d_x + alpha d_s.
+cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const float *d_s,
+                        const double *d_alpha, float *d_xt);
+cudaError_t i8_configure_kernels();
+cudaError_t i8_forward_max_pairs(int *pairs);
+cudaError_t i8_backward_max_pairs(int *pairs);
+cudaError_t i8_build_onehot(ccm_context *c);
+// tc_finalize over the loss partials of n_fwd_tiles 128-row forward tiles.
+cudaError_t launch_tc_finalize(ccm_context *c, const float *x1, float *d_g, long long n_fwd_tiles);
 // One CG trial on a tensor-core context: xt = x + alpha s (alpha on the device),
 // then the evaluation at xt, with the step fused into tc_prep.
 cudaError_t tc_evaluate_step(ccm_context *c, const float *d_x, const float *d_s,
@@ -155,6 +195,14 @@ struct ccm_context {
   int n_bwd_tiles = 0;
   ccm::FwdMaps fwd_maps;
   ccm::BwdMaps bwd_maps;
+
+  // integer tensor-core path
+  uint8_t *d_o1 = nullptr, *d_o128 = nullptr;          // Npad x S one-hot, values 1 / 128
+  int8_t *d_wdig[3] = {nullptr, nullptr, nullptr};     // S x S digits of W
+  int8_t *d_rdig[3] = {nullptr, nullptr, nullptr};     // Npad x S digits of R
+  uint32_t *d_colmax = nullptr;                        // 21 L column maxima of |W|
+  ccm::I8FwdMaps i8fwd_maps;
+  ccm::I8BwdMaps i8bwd_maps;
 
   // SIMT paths
   void *d_simt_pc = nullptr;      // N x 21 x L probabilities (float or double)

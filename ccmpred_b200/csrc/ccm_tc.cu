@@ -903,14 +903,19 @@ static cudaError_t launch_tc(ccm_context *c, const float *d_x, float *d_g,
         <<<2 * bwd_pairs, kBwdThreads, BwdSmem<NSPLIT>::kTotal, c->stream>>>(c->bwd_maps, ba);
   prof_mark(c);
 
-  FinalizeArgs za{};
-  za.part_f = c->d_part_f; za.n_part_f = (long long)fwd_tiles * 8;
-  za.part_reg = c->d_part_reg; za.n_part_reg = (long long)kQ * L;
-  za.x1 = x1; za.g1d = c->d_g1d; za.g1 = d_g; za.L = L; za.nsp = c->nsp;
-  za.lambda_single = c->lambda_single; za.lambda_pair = c->lambda_pair; za.out = c->d_out;
-  tc_finalize_kernel<<<1, 1024, 0, c->stream>>>(za);
+  launch_tc_finalize(c, x1, d_g, fwd_tiles);
   prof_mark(c);
   count_launch(c, 4);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tc_finalize(ccm_context *c, const float *x1, float *d_g, long long n_fwd_tiles) {
+  FinalizeArgs za{};
+  za.part_f = c->d_part_f; za.n_part_f = n_fwd_tiles * 8;
+  za.part_reg = c->d_part_reg; za.n_part_reg = (long long)kQ * c->L;
+  za.x1 = x1; za.g1d = c->d_g1d; za.g1 = d_g; za.L = c->L; za.nsp = c->nsp;
+  za.lambda_single = c->lambda_single; za.lambda_pair = c->lambda_pair; za.out = c->d_out;
+  tc_finalize_kernel<<<1, 1024, 0, c->stream>>>(za);
   return cudaGetLastError();
 }
 

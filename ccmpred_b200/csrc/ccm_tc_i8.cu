@@ -1,0 +1,968 @@
+// Integer tensor-core evaluation (CCM_PATH_TC_I8X3): the same two contractions as
+// the split-bf16 path (ccm_tc.cu), with 8-bit operands and exact 32-bit integer
+// accumulation on tcgen05 (kind::i8, cta_group::2).
+//
+// Fixed-point digits.  A value v with scale 2^e (|v| <= 2^e) is represented by the
+// integer Q = clamp(rint(v * 2^(21 - e)), -2^21, 2^21 - 1) and stored as three
+// bytes: d0 = Q >> 14 (signed, -128..127), d1 = (Q >> 7) & 127, d2 = Q & 127, so
+// that Q = d0 * 2^14 + d1 * 2^7 + d2.  The one-hot operand is stored twice, as
+// unsigned bytes 1 and 128, and the contractions accumulate
+//   hi = sum O1 * d0,   lo = sum O128 * d1 + sum O1 * d2 = sum O * (Q & 0x3fff)
+// in two s32 TMEM accumulators; sum O * Q = hi * 2^14 + lo exactly.  W takes one
+// power-of-two scale per coupling column (a, j) (its column maximum rounded up),
+// R = w (P - onehot), |R| < 1, takes the scale 1.  Quantisation error: at most
+// 2^-22 of the column scale per element; modelled against FP64 it gives a 3x
+// smaller gradient error than the hi+lo bf16 split, and the sums are exact.
+// Per K element the tensor cores do three 8-bit products (at twice the bf16
+// rate) where the split-bf16 path does two bf16 products: 3/4 of the cycles.
+//
+// One evaluation = colmax (+ the fused CG step), prep (digits of W, g2 <- 2 l2 x,
+// sum x^2), forward, backward, finalize (shared with ccm_tc.cu).
+#include <cuda_bf16.h>
+
+#include "ccm_internal.cuh"
+#include "ccm_layout.cuh"
+#include "ccm_ptx.cuh"
+
+namespace ccm {
+
+constexpr int kI8FracBits = 21;
+
+__device__ __forceinline__ uint8_t *i8_align1024(uint8_t *p) {
+  const uint32_t s = smem_u32(p);
+  return p + ((1024u - (s & 1023u)) & 1023u);
+}
+
+__device__ __forceinline__ void i8_record_error(int *status, int bit, int *abort_flag) {
+  atomicOr(status, bit);
+  *reinterpret_cast<volatile int *>(abort_flag) = 1;
+}
+
+__device__ __forceinline__ bool i8_aborted(const int *abort_flag) {
+  return *reinterpret_cast<const volatile int *>(abort_flag) != 0;
+}
+
+// 2^s as a float, s in [-126, 127].
+__device__ __forceinline__ float pow2f(int s) { return __int_as_float((s + 127) << 23); }
+
+// Smallest e with 2^e >= m for the float m with bits `mbits` (m >= 0), limited to
+// [-100, 127] so that 2^(21 - e) stays a normal float; 0 for m == 0.
+__device__ __forceinline__ int col_exponent(uint32_t mbits) {
+  if (mbits == 0) return 0;
+  const int E = (int)(mbits >> 23) - 127;
+  const int e = (mbits & 0x7FFFFFu) ? E + 1 : E;
+  return max(e, -100);
+}
+
+// The three digits of v at scale 2^e, given scale_in = 2^(21 - e).
+__device__ __forceinline__ void digits_of(float v, float scale_in, uint32_t &d0, uint32_t &d1,
+                                          uint32_t &d2) {
+  int q = __float2int_rn(v * scale_in);  // exact scaling by a power of two, one rounding
+  q = min(max(q, -(1 << kI8FracBits)), (1 << kI8FracBits) - 1);
+  d0 = (uint32_t)(q >> 14) & 0xFFu;
+  d1 = (uint32_t)(q >> 7) & 127u;
+  d2 = (uint32_t)q & 127u;
+}
+
+// ---------------------------------------------------------------- colmax
+// Column maxima of |W| over the 21 L rows (b, k), per coupling column c = a*L + j
+// (a < 21), as float bits with atomicMax (|v| >= 0 orders like its bits).  Block
+// (bx, by): 256 consecutive columns c of a 32 L row, rows [by*R, by*R + R).
+// STEP = true also takes the CG trial step: v = fmaf(alpha, s, x) is written to
+// xt for every element of x (the last row of blocks steps the single fields).
+template <bool STEP>
+__global__ void __launch_bounds__(256) i8_colmax_kernel(const float *__restrict__ x,
+                                                        const float *__restrict__ s,
+                                                        const double *__restrict__ alpha,
+                                                        float *__restrict__ xt,
+                                                        uint32_t *__restrict__ colmax, int L,
+                                                        long long nsp, int rows_per_block) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int w32 = kQPad * L;
+  float a = 0.0f;
+  if (STEP) {
+    a = (float)alpha[0];
+    if (blockIdx.y == gridDim.y - 1) {
+      if (c < nsp) xt[c] = fmaf(a, s[c], x[c]);
+      return;
+    }
+  }
+  if (c >= w32) return;
+  const int r0 = blockIdx.y * rows_per_block;
+  const int r1 = min(r0 + rows_per_block, kQ * L);
+  float m = 0.0f;
+  for (int r = r0; r < r1; ++r) {
+    const long long i = nsp + (long long)r * w32 + c;
+    float v = x[i];
+    if (STEP) {
+      v = fmaf(a, s[i], v);
+      xt[i] = v;
+    }
+    m = fmaxf(m, fabsf(v));
+  }
+  if (c < kQ * L && m > 0.0f) atomicMax(colmax + c, __float_as_uint(m));
+}
+
+// ---------------------------------------------------------------- prep
+// One block per row (b, k) of W, as tc_prep: g2 <- g2_coef * lambda2 * x, the FP64
+// partial of sum x^2, and row s(b, k) of the three digit matrices of Wperm (16
+// slots per thread, one 16-byte store per digit matrix).
+__global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ x2,
+                                                      float *__restrict__ g2, I8PrepArgs args) {
+  extern __shared__ __align__(16) float xrow[];  // 21 L floats
+  const int L = args.L;
+  const int row = blockIdx.x;
+  const int b = row / L, k = row % L;
+  const long long base = (long long)row * kQPad * L;
+  const float two_l2 = args.g2_coef * args.lambda_pair;
+  const int nreal = kQ * L;
+  double acc = 0.0;
+  if ((L & 3) == 0) {
+    const float4 *src = reinterpret_cast<const float4 *>(x2 + base);
+    float4 *dst = reinterpret_cast<float4 *>(g2 + base);
+    const int n4 = kQPad * L / 4, nreal4 = nreal / 4;
+    constexpr int kU = 4;
+    for (int i0 = threadIdx.x; i0 < n4; i0 += kU * blockDim.x) {
+      float4 v[kU];
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int i = i0 + u * blockDim.x;
+        v[u] = i < n4 ? __ldcs(src + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < kU; ++u) {
+        const int i = i0 + u * blockDim.x;
+        if (i < n4) {
+          acc += (double)v[u].x * v[u].x + (double)v[u].y * v[u].y + (double)v[u].z * v[u].z +
+                 (double)v[u].w * v[u].w;
+          if (i < nreal4) reinterpret_cast<float4 *>(xrow)[i] = v[u];
+          __stcs(dst + i, make_float4(two_l2 * v[u].x, two_l2 * v[u].y, two_l2 * v[u].z,
+                                      two_l2 * v[u].w));
+        }
+      }
+    }
+  } else {
+    for (int i = threadIdx.x; i < kQPad * L; i += blockDim.x) {
+      const float v = x2[base + i];
+      acc += (double)v * v;
+      if (i < nreal) xrow[i] = v;
+      g2[base + i] = two_l2 * v;
+    }
+  }
+  __syncthreads();
+  const long long srow = (long long)slot_of(b, k) * args.S;
+  for (int u = threadIdx.x; u < args.S / 16; u += blockDim.x) {
+    uint32_t p0[4], p1[4], p2[4];
+#pragma unroll
+    for (int e4 = 0; e4 < 4; ++e4) {
+      uint32_t h0 = 0, h1 = 0, h2 = 0;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int sl = u * 16 + e4 * 4 + e;
+        const int t = sl / kGroupSlots, r = sl % kGroupSlots;
+        uint32_t d0 = 0, d1 = 0, d2 = 0;
+        if (r < kGroupUsed) {
+          const int a = r / kGroupCols, j = t * kGroupCols + r % kGroupCols;
+          if (j < L) {
+            const int c = a * L + j;
+            digits_of(xrow[c], pow2f(kI8FracBits - col_exponent(__ldg(args.colmax + c))), d0,
+                      d1, d2);
+          }
+        }
+        h0 |= d0 << (8 * e);
+        h1 |= d1 << (8 * e);
+        h2 |= d2 << (8 * e);
+      }
+      p0[e4] = h0; p1[e4] = h1; p2[e4] = h2;
+    }
+    const long long off = srow + (long long)u * 16;
+    *reinterpret_cast<uint4 *>(args.wdig[0] + off) = make_uint4(p0[0], p0[1], p0[2], p0[3]);
+    *reinterpret_cast<uint4 *>(args.wdig[1] + off) = make_uint4(p1[0], p1[1], p1[2], p1[3]);
+    *reinterpret_cast<uint4 *>(args.wdig[2] + off) = make_uint4(p2[0], p2[1], p2[2], p2[3]);
+  }
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sum = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += red[w];
+    args.part_reg[row] = sum;
+  }
+}
+
+// One-hot operands of the integer path: O1[n][s] = 1 and O128[n][s] = 128 where
+// the state of column l(s) in row n is q(s), and in the ones slot of every real
+// row; 0 elsewhere.
+__global__ void i8_onehot_kernel(const uint8_t *__restrict__ msa, uint8_t *__restrict__ o1,
+                                 uint8_t *__restrict__ o128, int L, int N, int S, int Npad) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)Npad * S) return;
+  const int n = (int)(idx / S), s = (int)(idx % S);
+  const int t = s / kGroupSlots, r = s % kGroupSlots;
+  bool one = false;
+  if (n < N) {
+    if (s == kOnesSlot) {
+      one = true;
+    } else if (r < kGroupUsed) {
+      const int q = r / kGroupCols, l = t * kGroupCols + r % kGroupCols;
+      one = l < L && msa[(long long)n * L + l] == q;
+    }
+  }
+  o1[idx] = one ? 1 : 0;
+  o128[idx] = one ? 128 : 0;
+}
+
+}  // namespace ccm
+
+namespace ccm {
+
+// ---------------------------------------------------------------- forward
+// Pair tiles of 256 rows x 256 slots as in tc_forward.  Per tile the MMAs run in
+// two phases: first the low digits into `lo` (O128 x d1 + O1 x d2), then the high
+// digit into `hi` (O1 x d0).  The epilogue merges z = (hi * 2^14 + lo) * scale + V
+// into float logits written back over `hi`, releases `lo` (the next tile's low
+// phase may start), runs the softmax passes on `hi`, writes the digits of R and
+// releases `hi`.  TMEM: hi = columns [0, 256), lo = [256, 512).
+constexpr int kI8BM = 128, kI8PairM = 256, kI8BN = 256, kI8HalfN = 128, kI8FwdBK = 64;
+constexpr int kI8Threads = 320;
+
+struct I8FwdSmem {
+  static constexpr int kStages = 6;
+  static constexpr int kTile = kI8BM * kI8FwdBK;  // 8 KB: A 128 rows x 64 B, B 64 rows x 128 B
+  static constexpr int kOffA1 = 0;
+  static constexpr int kOffA128 = kTile;
+  static constexpr int kOffB = 2 * kTile;          // lo phase: d1, d2
+  // hi phase: two K blocks per stage: O1 (kb) at 0, O1 (kb+1) at kTile, d0 (kb) at
+  // 2 kTile, d0 (kb+1) at 3 kTile, so that a stage feeds four MMAs in both phases
+  static constexpr int kStage = 4 * kTile;
+  static constexpr int kBarOff = kStages * kStage;
+  static constexpr int kTabOff = kBarOff + 256;    // per tile: scale[256], V[256]
+  static constexpr int kXOff = kTabOff + 2 * kGroupSlots * 4;
+  static constexpr int kXBytes = 2 * kI8BM * 2 * kGroupCols * 4;  // (max, sum) per half
+  static constexpr int kTotal = kXOff + kXBytes + 1024;
+};
+
+// Epilogue of one tile for one warp (TMEM lane quarter q, column half H: columns
+// 128 H .. 128 H + 127 of the tile).  Three passes over TMEM, one exp per element:
+//   merge: z = (hi * 2^14 + lo) * scale + V (exact integer sum, one rounding),
+//          written over hi; per alignment column jj the maximum m of the own
+//          states and the logit of the observed state; then `lo` is released;
+//   B:     e = exp(z - m) written over z, s = sum e;
+//          (m, s) exchanged with the partner warp (same rows, other half):
+//          M = max(m, m'), S = s exp(m - M) + s' exp(m' - M) (same order in both
+//          halves), lse = M + log S;
+//   C:     P = e * exp(m - M) / S, R = w (P - onehot) as its three digits.
+template <int H>
+__device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint32_t t_hi,
+                                                     uint32_t t_lo, const float *tab_scale,
+                                                     const float *tab_v, float *xbuf, int q,
+                                                     int lane, int n, int t, long long part,
+                                                     uint32_t lo_bar) {
+  const int L = args.L;
+  const int j0 = t * kGroupCols;
+  const bool live = n < args.N;
+  const float wn = live ? args.w[n] : 0.0f;
+  const int row = q * 32 + lane;
+  const int pair_bar = 2 + q;
+  int xr[kGroupCols];
+#pragma unroll
+  for (int jj = 0; jj < kGroupCols; ++jj) {
+    const int j = j0 + jj;
+    xr[jj] = (live && j < L) ? (int)args.msa[(long long)n * L + j] : -1;
+  }
+  float mx[kGroupCols], tg[kGroupCols], se[kGroupCols];
+#pragma unroll
+  for (int jj = 0; jj < kGroupCols; ++jj) { mx[jj] = -INFINITY; tg[jj] = 0.0f; se[jj] = 0.0f; }
+  // merge + maxima
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int cc = 4 * H + c;
+    uint32_t vh[32], vl[32];
+    __syncwarp();
+    tmem_ld32(t_hi + cc * 32, vh);
+    tmem_ld32(t_lo + cc * 32, vl);
+    tmem_wait_ld();
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      const int col = cc * 32 + i;
+      const long long qs = (long long)(int)vh[i] * 16384 + (long long)(int)vl[i];
+      const float z = fmaf(__ll2float_rn(qs), tab_scale[col], tab_v[col]);
+      vh[i] = __float_as_uint(z);
+      if (col < kGroupUsed) {
+        const int a = col / kGroupCols, jj = col % kGroupCols;
+        mx[jj] = fmaxf(mx[jj], z);
+        if (xr[jj] == a) tg[jj] = z;
+      }
+    }
+    tmem_st32(t_hi + cc * 32, vh);
+  }
+  tmem_wait_st();
+  tc_fence_before();
+  __syncwarp();
+  if (lane == 0) mbar_arrive_cluster(lo_bar);  // the next tile's low phase may start
+  // B: e = exp(z - m), sum
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int cc = 4 * H + c;
+    uint32_t v[32];
+    __syncwarp();
+    tmem_ld32(t_hi + cc * 32, v);
+    tmem_wait_ld();
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      const int col = cc * 32 + i;
+      if (col < kGroupUsed) {
+        const int jj = col % kGroupCols;
+        const float e = expf(__uint_as_float(v[i]) - mx[jj]);
+        se[jj] += e;
+        v[i] = __float_as_uint(e);
+      }
+    }
+    tmem_st32(t_hi + cc * 32, v);
+  }
+  float *mine = xbuf + (H * kI8BM + row) * (2 * kGroupCols);
+  const float *other = xbuf + ((1 - H) * kI8BM + row) * (2 * kGroupCols);
+#pragma unroll
+  for (int jj = 0; jj < kGroupCols; ++jj) {
+    mine[jj] = mx[jj];
+    mine[kGroupCols + jj] = se[jj];
+  }
+  named_bar_sync(pair_bar, 64);
+  double floss = 0.0;
+  float cf[kGroupCols];
+#pragma unroll
+  for (int jj = 0; jj < kGroupCols; ++jj) {
+    const float mo = other[jj], so = other[kGroupCols + jj];
+    const float M = fmaxf(mx[jj], mo);
+    const float fa = expf(mx[jj] - M), fo = expf(mo - M);
+    const float S = H == 0 ? se[jj] * fa + so * fo : so * fo + se[jj] * fa;
+    const float lse = M + logf(S);
+    cf[jj] = fa / S;
+    if (xr[jj] >= 0 && ((xr[jj] * kGroupCols + jj) >> 7) == H)
+      floss += (double)(wn * (lse - tg[jj]));
+  }
+  tmem_wait_st();
+  // C: R = w (P - onehot), three digits per element
+  const long long rbase = (long long)n * args.S + (long long)t * kGroupSlots;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int cc = 4 * H + c;
+    uint32_t v[32];
+    __syncwarp();
+    tmem_ld32(t_hi + cc * 32, v);
+    tmem_wait_ld();
+    uint32_t w0[8], w1[8], w2[8];
+#pragma unroll
+    for (int e4 = 0; e4 < 8; ++e4) {
+      uint32_t h0 = 0, h1 = 0, h2 = 0;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int i = e4 * 4 + e;
+        const int col = cc * 32 + i;
+        float r = 0.0f;
+        if (col < kGroupUsed) {
+          const int a = col / kGroupCols, jj = col % kGroupCols;
+          if (xr[jj] >= 0)
+            r = wn * (__uint_as_float(v[i]) * cf[jj] - (xr[jj] == a ? 1.0f : 0.0f));
+        }
+        uint32_t d0, d1, d2;
+        digits_of(r, (float)(1 << kI8FracBits), d0, d1, d2);
+        h0 |= d0 << (8 * e);
+        h1 |= d1 << (8 * e);
+        h2 |= d2 << (8 * e);
+      }
+      w0[e4] = h0; w1[e4] = h1; w2[e4] = h2;
+    }
+    const long long off = rbase + cc * 32;
+    st_global_v8(args.r[0] + off, w0);
+    st_global_v8(args.r[1] + off, w1);
+    st_global_v8(args.r[2] + off, w2);
+  }
+  for (int o = 16; o > 0; o >>= 1) floss += __shfl_xor_sync(0xffffffffu, floss, o);
+  if (lane == 0) args.part_f[part * 8 + H * 4 + q] = floss;
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
+    i8_forward_kernel(const __grid_constant__ I8FwdMaps maps, I8FwdArgs args) {
+  using SM = I8FwdSmem;
+  constexpr int kStages = SM::kStages;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = i8_align1024(smem_raw);
+  // full[] and the *_empty barriers are used in the leader only; empty[] and
+  // acc_full in both CTAs (the leader's commits reach both)
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + SM::kBarOff);
+  uint64_t *empty = full + kStages;
+  uint64_t *acc_full = empty + kStages;
+  uint64_t *lo_empty = acc_full + 1;
+  uint64_t *hi_empty = lo_empty + 1;
+  uint64_t *drain = hi_empty + 1;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+  float *tab_scale = reinterpret_cast<float *>(smem + SM::kTabOff);
+  float *tab_v = tab_scale + kGroupSlots;
+  float *xbuf = reinterpret_cast<float *>(smem + SM::kXOff);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+  const int n_tiles = args.m_tiles * args.T;
+  const int k_blocks = args.S / kI8FwdBK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+    mbar_init(acc_full, 1);
+    mbar_init(lo_empty, 16);
+    mbar_init(hi_empty, 16);
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&maps.a1);
+    prefetch_tmap(&maps.a128);
+    for (int i = 0; i < 3; ++i) prefetch_tmap(&maps.b[i]);
+  }
+  if (warp == 1) { tmem_alloc_pair(tmem_slot, 512); tmem_relinquish_pair(); }
+  tc_fence_before();
+  cluster_sync();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  const uint32_t t_hi = tmem_base, t_lo = tmem_base + kI8BN;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---------------- TMA producer (both CTAs), in the MMA's order
+      uint32_t it = 0;
+      bool ok = true;
+      for (int tile = pair; tile < n_tiles && ok && !i8_aborted(abort_flag); tile += npairs) {
+        const int m = tile % args.m_tiles, t = tile / args.m_tiles;
+        const int row0 = m * kI8PairM + (int)rank * kI8BM;
+        const int col0 = t * kI8BN + (int)rank * kI8HalfN;
+        for (int phase = 0; phase < 2 && ok; ++phase) {  // 0: low digits, 1: high digit
+          for (int kb = 0; kb < k_blocks; kb += (phase == 0 ? 1 : 2), ++it) {
+            const int stage = it % kStages;
+            const uint32_t round = it / kStages;
+            if (!mbar_wait(&empty[stage], (round & 1) ^ 1)) {
+              i8_record_error(args.status, kErrFwdTimeout, abort_flag);
+              ok = false;
+              break;
+            }
+            uint8_t *st = smem + stage * SM::kStage;
+            const uint32_t fb = mapa_shared(smem_u32(&full[stage]), 0);
+            const int kx = kb * kI8FwdBK;
+            if (phase == 0) {
+              if (rank == 0) mbar_arrive_expect_tx(&full[stage], 2 * 4 * SM::kTile);
+              tma_load_2d_pair(st + SM::kOffA1, &maps.a1, fb, kx, row0);
+              tma_load_2d_pair(st + SM::kOffA128, &maps.a128, fb, kx, row0);
+              tma_load_2d_pair(st + SM::kOffB, &maps.b[1], fb, col0, kx);
+              tma_load_2d_pair(st + SM::kOffB + SM::kTile, &maps.b[2], fb, col0, kx);
+            } else {
+              if (rank == 0) mbar_arrive_expect_tx(&full[stage], 2 * 4 * SM::kTile);
+              tma_load_2d_pair(st, &maps.a1, fb, kx, row0);
+              tma_load_2d_pair(st + SM::kTile, &maps.a1, fb, kx + kI8FwdBK, row0);
+              tma_load_2d_pair(st + 2 * SM::kTile, &maps.b[0], fb, col0, kx);
+              tma_load_2d_pair(st + 3 * SM::kTile, &maps.b[0], fb, col0, kx + kI8FwdBK);
+            }
+          }
+        }
+      }
+      const uint32_t issued = it;
+      for (uint32_t r = (issued > kStages ? issued - kStages : 0); r < issued; ++r) {
+        const bool w = rank == 0 ? mbar_wait(&full[r % kStages], (r / kStages) & 1)
+                                 : mbar_wait(&empty[r % kStages], (r / kStages) & 1);
+        if (!w) {
+          i8_record_error(args.status, kErrFwdTimeout, abort_flag);
+          break;
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && rank == 0) {
+      // ---------------- MMA issuer (leader): 256 x 256 x 32 pair MMAs, u8 x s8 -> s32
+      constexpr uint32_t idesc = idesc_i8_s32(kI8PairM, kI8BN, 0, 1, 0, 1);
+      uint32_t it = 0;
+      int local = 0;
+      bool ok = true;
+      for (int tile = pair; tile < n_tiles && ok && !i8_aborted(abort_flag);
+           tile += npairs, ++local) {
+        const uint32_t wpar = (local & 1) ^ 1;
+        for (int phase = 0; phase < 2 && ok; ++phase) {
+          if (!mbar_wait(phase == 0 ? lo_empty : hi_empty, wpar)) {
+            i8_record_error(args.status, kErrFwdTimeout, abort_flag);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          for (int kb = 0; kb < k_blocks; kb += (phase == 0 ? 1 : 2), ++it) {
+            const int stage = it % kStages;
+            const uint32_t round = it / kStages;
+            if (!mbar_wait(&full[stage], round & 1)) {
+              i8_record_error(args.status, kErrFwdTimeout, abort_flag);
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t s0 = smem_u32(smem + stage * SM::kStage);
+#pragma unroll
+            for (int k32 = 0; k32 < kI8FwdBK / 32; ++k32) {
+              if (phase == 0) {
+                const uint64_t a1 = sdesc_sw64(s0 + SM::kOffA1 + k32 * 32, 16, 512);
+                const uint64_t a128 = sdesc_sw64(s0 + SM::kOffA128 + k32 * 32, 16, 512);
+                const uint64_t bA = sdesc_sw128(s0 + SM::kOffB + k32 * 32 * 128, SM::kTile, 1024);
+                const uint64_t bB =
+                    sdesc_sw128(s0 + SM::kOffB + SM::kTile + k32 * 32 * 128, SM::kTile, 1024);
+                umma_i8_pair(t_lo, a128, bA, idesc, (kb | k32) != 0);
+                umma_i8_pair(t_lo, a1, bB, idesc, 1);
+              } else {
+#pragma unroll
+                for (int sub = 0; sub < 2; ++sub) {
+                  const uint64_t a1 = sdesc_sw64(s0 + sub * SM::kTile + k32 * 32, 16, 512);
+                  const uint64_t b0 = sdesc_sw128(s0 + (2 + sub) * SM::kTile + k32 * 32 * 128,
+                                                  SM::kTile, 1024);
+                  umma_i8_pair(t_hi, a1, b0, idesc, (kb | sub | k32) != 0);
+                }
+              }
+            }
+            umma_commit_pair(&empty[stage], 0x3);
+          }
+        }
+        if (ok) umma_commit_pair(acc_full, 0x3);
+      }
+      umma_commit_pair(drain, 0x1);
+      if (!mbar_wait(drain, 0)) i8_record_error(args.status, kErrFwdTimeout, abort_flag);
+    }
+  } else {
+    // ---------------- epilogue (both CTAs): 8 warps, lane quarter q, column half
+    const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
+    const int ethr = threadIdx.x - 64;
+    const int L = args.L;
+    const uint32_t lo_bar = mapa_shared(smem_u32(lo_empty), 0);
+    const uint32_t hi_bar = mapa_shared(smem_u32(hi_empty), 0);
+    int local = 0;
+    for (int tile = pair; tile < n_tiles; tile += npairs, ++local) {
+      // all eight warps finished the previous tile (tables free) and saw no abort
+      if (named_bar_or(1, 256, i8_aborted(abort_flag))) break;
+      const int m = tile % args.m_tiles, t = tile / args.m_tiles;
+      {
+        // slot tables of this tile: merge scale 2^(e - 21) and the single field V
+        const int r = ethr;
+        float sc = 0.0f, vv = 0.0f;
+        if (r < kGroupUsed) {
+          const int a = r / kGroupCols, j = t * kGroupCols + r % kGroupCols;
+          if (j < L) {
+            sc = pow2f(col_exponent(args.colmax[a * L + j]) - kI8FracBits);
+            if (a < kQ - 1) vv = args.x1[a * L + j];
+          }
+        }
+        tab_scale[r] = sc;
+        tab_v[r] = vv;
+      }
+      named_bar_sync(1, 256);
+      const int n = m * kI8PairM + (int)rank * kI8BM + q * 32 + lane;
+      const bool ok = mbar_wait(acc_full, local & 1);
+      if (__any_sync(0xffffffffu, !ok)) {
+        if (lane == 0) i8_record_error(args.status, kErrFwdTimeout, abort_flag);
+        continue;
+      }
+      tc_fence_after();
+      const uint32_t lq = (uint32_t)(q * 32) << 16;
+      const long long part = (long long)tile * 2 + rank;
+      if (half == 0)
+        i8_fwd_epilogue_tile<0>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v, xbuf, q, lane, n, t,
+                                part, lo_bar);
+      else
+        i8_fwd_epilogue_tile<1>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v, xbuf, q, lane, n, t,
+                                part, lo_bar);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(hi_bar);
+    }
+  }
+
+  tc_fence_before();
+  cluster_sync();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc_pair(tmem_base, 512);
+  }
+}
+
+}  // namespace ccm
+
+namespace ccm {
+
+// ---------------------------------------------------------------- backward
+// Pair tiles of 256 x 256 slots (P <= Q for the symmetric gradient) as in
+// tc_backward.  Per K step of 32 rows, with the digits r0..r2 of R and the two
+// one-hot operands O1, O128 (both sides MN-major, 8-bit):
+//   hi += O1_P^T r0_Q + r0_P^T O1_Q
+//   lo += O128_P^T r1_Q + O1_P^T r2_Q + r1_P^T O128_Q + r2_P^T O1_Q
+// (SYM = false: the O^T R products only).  The sums are exact in s32 for up to
+// 32768 rows; longer alignments are cut into K chunks of that length, each merged
+// as (hi * 2^14 + lo) * 2^-21 (exact, one rounding) into FP32 registers.  The
+// output phase is tc_backward's: one atomic add per g2 element.
+constexpr int kI8BwdBK = 32;
+constexpr int kI8BwdChunkKB = 1024;  // 32768 rows: |lo| <= 32768 * 2 * 16383 < 2^31
+
+struct I8BwdSmem {
+  static constexpr int kStages = 5;
+  static constexpr int kTile = 128 * kI8BwdBK;  // 4 KB: 128 slots x 32 rows, 8-bit
+  // P side: O1, O128, r0, r1, r2 (this CTA's 128 P slots); Q side: the same (its 128 Q slots)
+  static constexpr int kStage = 10 * kTile;
+  static constexpr int kBarOff = kStages * kStage;
+  static constexpr int kTOff = kBarOff + 256;
+  static constexpr int kTBytes = 8 * 32 * 9 * 4;
+  static constexpr int kTotal = kTOff + kTBytes + 1024;
+};
+
+template <bool SYM>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
+    i8_backward_kernel(const __grid_constant__ I8BwdMaps maps, BwdArgs args) {
+  using SM = I8BwdSmem;
+  constexpr int kStages = SM::kStages;
+  constexpr int kBN = 256, kHalfN = 128, kPairM = 256, kBM = 128;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = i8_align1024(smem_raw);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + SM::kBarOff);
+  uint64_t *empty = full + kStages;
+  uint64_t *acc_full = empty + kStages;
+  uint64_t *acc_empty = acc_full + 1;
+  uint64_t *drain = acc_empty + 1;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+  const int n_tiles = args.n_tiles;
+  const int k_blocks = args.Npad / kI8BwdBK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, 16);
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&maps.o1);
+    prefetch_tmap(&maps.o128);
+    for (int i = 0; i < 3; ++i) prefetch_tmap(&maps.r[i]);
+  }
+  if (warp == 1) { tmem_alloc_pair(tmem_slot, 512); tmem_relinquish_pair(); }
+  tc_fence_before();
+  cluster_sync();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  const uint32_t t_hi = tmem_base, t_lo = tmem_base + kBN;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t it = 0;
+      bool ok = true;
+      for (int tile = pair; tile < n_tiles && ok && !i8_aborted(abort_flag); tile += npairs) {
+        const int2 pq = args.tiles[tile];
+        const int xP = pq.x * kPairM + (int)rank * kBM;
+        const int xQ = pq.y * kBN + (int)rank * kHalfN;
+        for (int kb = 0; kb < k_blocks; ++kb, ++it) {
+          const int stage = it % kStages;
+          const uint32_t round = it / kStages;
+          if (!mbar_wait(&empty[stage], (round & 1) ^ 1)) {
+            i8_record_error(args.status, kErrBwdTimeout, abort_flag);
+            ok = false;
+            break;
+          }
+          uint8_t *st = smem + stage * SM::kStage;
+          const int y = kb * kI8BwdBK;
+          const uint32_t fb = mapa_shared(smem_u32(&full[stage]), 0);
+          if (rank == 0) mbar_arrive_expect_tx(&full[stage], 2 * (SYM ? 10 : 5) * SM::kTile);
+          tma_load_2d_pair(st + 0 * SM::kTile, &maps.o1, fb, xP, y);
+          tma_load_2d_pair(st + 1 * SM::kTile, &maps.o128, fb, xP, y);
+          if (SYM)
+            for (int i = 0; i < 3; ++i)
+              tma_load_2d_pair(st + (2 + i) * SM::kTile, &maps.r[i], fb, xP, y);
+          if (SYM) {
+            tma_load_2d_pair(st + 5 * SM::kTile, &maps.o1, fb, xQ, y);
+            tma_load_2d_pair(st + 6 * SM::kTile, &maps.o128, fb, xQ, y);
+          }
+          for (int i = 0; i < 3; ++i)
+            tma_load_2d_pair(st + (7 + i) * SM::kTile, &maps.r[i], fb, xQ, y);
+        }
+      }
+      const uint32_t issued = it;
+      for (uint32_t r = (issued > (uint32_t)kStages ? issued - kStages : 0); r < issued; ++r) {
+        const bool w = rank == 0 ? mbar_wait(&full[r % kStages], (r / kStages) & 1)
+                                 : mbar_wait(&empty[r % kStages], (r / kStages) & 1);
+        if (!w) {
+          i8_record_error(args.status, kErrBwdTimeout, abort_flag);
+          break;
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && rank == 0) {
+      constexpr uint32_t id_us = idesc_i8_s32(kPairM, kBN, 0, 1, 1, 1);  // A = one-hot, B = R
+      constexpr uint32_t id_su = idesc_i8_s32(kPairM, kBN, 1, 0, 1, 1);  // A = R, B = one-hot
+      uint32_t it = 0, chunk = 0;
+      bool ok = true;
+      for (int tile = pair; tile < n_tiles && ok && !i8_aborted(abort_flag); tile += npairs) {
+        for (int kb0 = 0; kb0 < k_blocks && ok; kb0 += kI8BwdChunkKB, ++chunk) {
+          if (!mbar_wait(acc_empty, (chunk & 1) ^ 1)) {
+            i8_record_error(args.status, kErrBwdTimeout, abort_flag);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const int kb1 = min(kb0 + kI8BwdChunkKB, k_blocks);
+          for (int kb = kb0; kb < kb1; ++kb, ++it) {
+            const int stage = it % kStages;
+            const uint32_t round = it / kStages;
+            if (!mbar_wait(&full[stage], round & 1)) {
+              i8_record_error(args.status, kErrBwdTimeout, abort_flag);
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t s0 = smem_u32(smem + stage * SM::kStage);
+            auto d = [&](int i) { return sdesc_sw128(s0 + i * SM::kTile, SM::kTile, 1024); };
+            const uint32_t first = kb == kb0 ? 0u : 1u;
+            umma_i8_pair(t_hi, d(0), d(7), id_us, first);  // O1_P^T r0_Q
+            umma_i8_pair(t_lo, d(1), d(8), id_us, first);  // O128_P^T r1_Q
+            umma_i8_pair(t_lo, d(0), d(9), id_us, 1);      // O1_P^T r2_Q
+            if (SYM) {
+              umma_i8_pair(t_hi, d(2), d(5), id_su, 1);    // r0_P^T O1_Q
+              umma_i8_pair(t_lo, d(3), d(6), id_su, 1);    // r1_P^T O128_Q
+              umma_i8_pair(t_lo, d(4), d(5), id_su, 1);    // r2_P^T O1_Q
+            }
+            umma_commit_pair(&empty[stage], 0x3);
+          }
+          if (!ok) break;
+          umma_commit_pair(acc_full, 0x3);
+        }
+      }
+      umma_commit_pair(drain, 0x1);
+      if (!mbar_wait(drain, 0)) i8_record_error(args.status, kErrBwdTimeout, abort_flag);
+    }
+  } else {
+    // Epilogue: as tc_backward, with each K chunk merged from the two integer
+    // accumulators (16 columns per TMEM load) into FP32 registers.
+    const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
+    const int L = args.L;
+    float *__restrict__ g2 = args.g2;
+    float *Tb = reinterpret_cast<float *>(smem + SM::kTOff) + (warp - 2) * 32 * 9;
+    const uint32_t empty_bar = mapa_shared(smem_u32(acc_empty), 0);
+    uint32_t chunk = 0;
+    bool ok = true;
+    for (int tile = pair; tile < n_tiles && ok; tile += npairs) {
+      float accv[kHalfN];
+#pragma unroll
+      for (int i = 0; i < kHalfN; ++i) accv[i] = 0.0f;
+      for (int kb0 = 0; kb0 < k_blocks; kb0 += kI8BwdChunkKB, ++chunk) {
+        const bool w_ok = mbar_wait(acc_full, chunk & 1);
+        if (__any_sync(0xffffffffu, !w_ok)) {
+          if (lane == 0) i8_record_error(args.status, kErrBwdTimeout, abort_flag);
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t col0 = half * kHalfN + ((uint32_t)(q * 32) << 16);
+#pragma unroll
+        for (int c = 0; c < kHalfN / 16; ++c) {
+          uint32_t vh[16], vl[16];
+          __syncwarp();
+          tmem_ld16(t_hi + col0 + c * 16, vh);
+          tmem_ld16(t_lo + col0 + c * 16, vl);
+          tmem_wait_ld();
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const long long qs = (long long)(int)vh[i] * 16384 + (long long)(int)vl[i];
+            accv[c * 16 + i] += (float)((double)qs * 4.76837158203125e-07);  // 2^-21
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive_cluster(empty_bar);
+      }
+      if (!ok) break;
+
+      const int2 pq = args.tiles[tile];
+      const int rowbase = pq.x * kPairM + (int)rank * kBM + q * 32;
+      const int s1 = rowbase + lane;
+      const int t1 = s1 / kGroupSlots, r1 = s1 % kGroupSlots;
+      const int b = r1 / kGroupCols, k = t1 * kGroupCols + r1 % kGroupCols;
+      const bool valid1 = r1 < kGroupUsed && k < L;
+      const long long colt = (long long)b * L + k;
+      const int tQ = pq.y * kBN / kGroupSlots;
+      const int rQ = pq.y * kBN % kGroupSlots + half * kHalfN;
+      const int sQ = tQ * kGroupSlots + rQ;
+#pragma unroll
+      for (int cb = 0; cb < kHalfN / 8; ++cb) {
+        __syncwarp();
+#pragma unroll
+        for (int e = 0; e < 8; ++e) Tb[lane * 9 + e] = accv[cb * 8 + e];
+        __syncwarp();
+        if (SYM) {
+#pragma unroll 1
+          for (int col = 0; col < 8; ++col) {
+            const int r2 = rQ + cb * 8 + col;
+            const int s2 = sQ + cb * 8 + col;
+            const int a = r2 / kGroupCols, j = tQ * kGroupCols + r2 % kGroupCols;
+            const bool valid2 = r2 < kGroupUsed && j < L;
+            if (s1 < s2) {
+              const float val = Tb[lane * 9 + col];
+              if (valid1 && valid2) {
+                if (k != j) atomicAdd(g2 + ((long long)a * L + j) * kQPad * L + colt, val);
+              } else if (s2 == kOnesSlot && valid1 && b < kQ - 1) {
+                args.g1d[b * L + k] = val;
+              }
+            }
+          }
+        }
+        const int col = lane & 7;
+        const int r2 = rQ + cb * 8 + col;
+        const int s2 = sQ + cb * 8 + col;
+        const int a = r2 / kGroupCols, j = tQ * kGroupCols + r2 % kGroupCols;
+        const bool valid2 = r2 < kGroupUsed && j < L;
+#pragma unroll
+        for (int it = 0; it < 8; ++it) {
+          const int row = 4 * it + (lane >> 3);
+          const int s1r = rowbase + row;
+          if (SYM && s1r > s2) continue;
+          const float val = Tb[row * 9 + col];
+          const int tr = s1r / kGroupSlots, rr = s1r % kGroupSlots;
+          const int br = rr / kGroupCols, kr = tr * kGroupCols + rr % kGroupCols;
+          if (rr < kGroupUsed && kr < L) {
+            if (valid2 && (!SYM || kr != j)) atomicAdd(g2 + x2_index(br, kr, a, j, L), val);
+          } else if (s1r == kOnesSlot && valid2 && a < kQ - 1) {
+            args.g1d[a * L + j] = val;
+          }
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  cluster_sync();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc_pair(tmem_base, 512);
+  }
+}
+
+}  // namespace ccm
+
+namespace ccm {
+
+// ---------------------------------------------------------------- launchers
+// Evaluation at d_x, or, with d_s, at d_xt = d_x + alpha d_s (the step is taken
+// by the column-max pass, which writes d_xt).  Profile marks: [colmax + prep |
+// forward | backward | finalize].
+cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const float *d_s,
+                        const double *d_alpha, float *d_xt) {
+  const int L = c->L;
+  const bool step = d_s != nullptr;
+  const float *xe = step ? d_xt : d_x;
+  const float *x1 = xe;
+  const float *x2 = xe + c->nsp;
+  float *g2 = d_g + c->nsp;
+  cudaError_t e;
+
+  prof_mark(c);
+  if ((e = cudaMemsetAsync(c->d_colmax, 0, sizeof(uint32_t) * kQ * L, c->stream)) != cudaSuccess)
+    return e;
+  constexpr int kRows = 32;
+  const dim3 cgrid((kQPad * L + 255) / 256, (kQ * L + kRows - 1) / kRows + (step ? 1 : 0));
+  if (step)
+    i8_colmax_kernel<true><<<cgrid, 256, 0, c->stream>>>(d_x, d_s, d_alpha, d_xt, c->d_colmax,
+                                                          L, c->nsp, kRows);
+  else
+    i8_colmax_kernel<false><<<cgrid, 256, 0, c->stream>>>(d_x, nullptr, nullptr, nullptr,
+                                                           c->d_colmax, L, c->nsp, kRows);
+  I8PrepArgs pa{};
+  for (int i = 0; i < 3; ++i) pa.wdig[i] = c->d_wdig[i];
+  pa.colmax = c->d_colmax;
+  pa.part_reg = c->d_part_reg;
+  pa.L = L; pa.S = c->S; pa.lambda_pair = c->lambda_pair;
+  pa.g2_coef = c->gradient == CCM_GRADIENT_PARTIAL ? 1.0f : 2.0f;
+  i8_prep_kernel<<<kQ * L, 256, sizeof(float) * kQ * L, c->stream>>>(x2, g2, pa);
+  prof_mark(c);
+
+  I8FwdArgs fa{};
+  fa.msa = c->d_msa; fa.w = c->d_w; fa.x1 = x1; fa.colmax = c->d_colmax;
+  for (int i = 0; i < 3; ++i) fa.r[i] = c->d_rdig[i];
+  fa.part_f = c->d_part_f; fa.status = c->d_status;
+  fa.L = L; fa.N = c->N; fa.S = c->S; fa.T = c->T; fa.Npad = c->Npad;
+  fa.m_tiles = c->Npad / kI8PairM;
+  const int pair_tiles = fa.m_tiles * c->T;
+  const int fpairs = pair_tiles < c->fwd_pairs ? pair_tiles : c->fwd_pairs;
+  i8_forward_kernel<<<2 * fpairs, kI8Threads, I8FwdSmem::kTotal, c->stream>>>(c->i8fwd_maps, fa);
+  prof_mark(c);
+
+  BwdArgs ba{};
+  ba.x2 = x2; ba.g2 = g2; ba.g1d = c->d_g1d; ba.tiles = c->d_bwd_tiles;
+  ba.n_tiles = c->n_bwd_tiles; ba.status = c->d_status; ba.L = L; ba.S = c->S; ba.Npad = c->Npad;
+  ba.lambda_pair = c->lambda_pair;
+  const int bpairs = c->n_bwd_tiles < c->bwd_pairs ? c->n_bwd_tiles : c->bwd_pairs;
+  if (c->gradient == CCM_GRADIENT_PARTIAL)
+    i8_backward_kernel<false>
+        <<<2 * bpairs, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
+  else
+    i8_backward_kernel<true>
+        <<<2 * bpairs, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
+  prof_mark(c);
+
+  launch_tc_finalize(c, x1, d_g, 2LL * pair_tiles);
+  prof_mark(c);
+  count_launch(c, 5);
+  return cudaGetLastError();
+}
+
+cudaError_t i8_configure_kernels() {
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(i8_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                168000)) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(i8_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                I8FwdSmem::kTotal)) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(i8_backward_kernel<true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                I8BwdSmem::kTotal)) != cudaSuccess)
+    return e;
+  return cudaFuncSetAttribute(i8_backward_kernel<false>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, I8BwdSmem::kTotal);
+}
+
+cudaError_t i8_forward_max_pairs(int *pairs) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2, 1, 1);
+  cfg.blockDim = dim3(kI8Threads, 1, 1);
+  cfg.dynamicSmemBytes = I8FwdSmem::kTotal;
+  *pairs = 0;
+  return cudaOccupancyMaxActiveClusters(pairs, i8_forward_kernel, &cfg);
+}
+
+cudaError_t i8_backward_max_pairs(int *pairs) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2, 1, 1);
+  cfg.blockDim = dim3(kI8Threads, 1, 1);
+  cfg.dynamicSmemBytes = I8BwdSmem::kTotal;
+  *pairs = 0;
+  return cudaOccupancyMaxActiveClusters(pairs, i8_backward_kernel<true>, &cfg);
+}
+
+// One-hot operands for a context of the integer path (Npad x S bytes each).
+cudaError_t i8_build_onehot(ccm_context *c) {
+  const long long total = (long long)c->Npad * c->S;
+  i8_onehot_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c->stream>>>(
+      c->d_msa, c->d_o1, c->d_o128, c->L, c->N, c->S, c->Npad);
+  return cudaGetLastError();
+}
+
+}  // namespace ccm

@@ -59,6 +59,8 @@ extern "C" {
 #define CCM_PATH_TC_BF16X3 1 /* tcgen05, three bf16 terms (hi+mid+lo) */
 #define CCM_PATH_SIMT_F32 2  /* plain FP32 CUDA-core path (no tensor cores) */
 #define CCM_PATH_SIMT_F64 3  /* FP64 CUDA-core path (gradient checks) */
+#define CCM_PATH_TC_I8X3 4   /* tcgen05 kind::i8: W and R as three 8-bit fixed-point digits
+                                (21 fractional bits), exact s32 accumulation */
 
 /* gradient conventions */
 #define CCM_GRADIENT_TIED 0    /* the reference's g: coupling part along the tied direction
