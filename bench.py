@@ -56,15 +56,35 @@ PATH_ARITHMETIC = {
                "f64 loss/regulariser reductions",
 }
 
+
+_JSON_FD = None
+
+
+def quiet_stdout():
+    """Route everything written to stdout -- Python's prints and the C libraries'
+    printf (the reference's init prints its reweighting summary) -- to stderr, so
+    that the original stdout carries exactly the one JSON line (see emit)."""
+    global _JSON_FD
+    sys.stdout.flush()
+    _JSON_FD = os.dup(1)
+    os.dup2(2, 1)
+
+
+def emit(obj):
+    fd = _JSON_FD if _JSON_FD is not None else 1
+    os.write(fd, (json.dumps(obj) + "\n").encode())
+
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--path", default="tc_bf16x2", choices=["tc_bf16x2", "tc_bf16x3", "tc_i8x3"])
+    p.add_argument("--path", default="tc_i8x3", choices=["tc_i8x3", "tc_bf16x2", "tc_bf16x3"])
     p.add_argument("--e2e-steps", type=int, default=50)
     p.add_argument("--plain-steps", type=int, default=20)
+    p.add_argument("--compare-steps", type=int, default=300,
+                   help="evaluations of the split-bf16 path timed beside the default path")
     p.add_argument("--cpu-budget-s", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-precision", action="store_true")
@@ -216,7 +236,7 @@ def run_reference_arm(args, world, rank):
     from oracle import oracle as O
     cfg, msa, x = workload()
     if not O.ref_available():
-        print(json.dumps({"impl": "reference", "unavailable":
+        emit(({"impl": "reference", "unavailable":
                           "oracle/_ref/libccmref.so (reference CPU sources) was not built"}))
         return
     N, L = msa.shape
@@ -230,7 +250,7 @@ def run_reference_arm(args, world, rank):
     ev.close()
     value = args.steps / el
     cores = os.cpu_count() or 1
-    print(json.dumps({
+    emit(({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -247,7 +267,8 @@ def run_reference_arm(args, world, rank):
 def precision_block(msa, w, x, g_gpu, f_gpu, L):
     from ccmpred_b200 import nsingle_padded
     from oracle import oracle as O
-    f64, g64 = O.oracle_evaluate(msa, w, 0.01, 0.2 * (L - 1), x)
+    # lambda2 as the evaluators compute it (the reference's float 0.2f * (L - 1))
+    f64, g64 = O.oracle_evaluate(msa, w, 0.01, float(np.float32(0.2) * np.float32(L - 1)), x)
     d = g_gpu.astype(np.float64) - g64
     nsp, ns = nsingle_padded(L), 20 * L
     n = np.linalg.norm
@@ -327,13 +348,13 @@ def run_batch(args, world, rank, local):
     plain_total = float(np.sum(plain_t) * len(msas) / k)
     its = np.array([r.iterations for r in res])
     ok = sum(r.status in (0, -1023) for r in res)
-    print(json.dumps({
+    emit(({
         "metric": "MSAs/s, 256 ragged alignments solved to convergence", "value": value,
         "unit": "MSAs/s", "n_gpus": world, "higher_is_better": True, "scaling": "weak",
         "data": "synthetic", "dtype": "bf16",
         "config": {"workload": "batch256: L~U[50,400], N~logU[200,20000], seeds 1000+i, "
                                "eps 1e-3 or 250 iterations",
-                   "workers": args.batch_workers, "path": "tc_bf16x2"},
+                   "workers": args.batch_workers, "path": "tc_i8x3"},
         "wall_s": el, "solved_ok": ok, "iterations_mean": float(its.mean()),
         "plain_f32_one_at_a_time": {
             "msas_per_s_extrapolated": len(msas) / plain_total,
@@ -345,6 +366,7 @@ def run_batch(args, world, rank, local):
 
 def main():
     args = parse_args()
+    quiet_stdout()
     world, rank, local = dist_init(args)
     if args.impl == "b200" and args.workload == "batch256":
         run_batch(args, world, rank, local)
@@ -447,6 +469,31 @@ def main():
                     "tc_backward": T * (T + 1) / 2 * 256 * 256 * 2.0 * Npad * 2 * nsplit}[dom]
         executed_tf = executed / (dom_ms / 1e3) / 1e12
 
+        other = None
+        if args.compare_steps > 0 and world == 1 and args.path != "tc_bf16x2":
+            # the split-bf16 tensor-core path on the same inputs, same timing method
+            be = cb.Evaluator(msa, weights=w, path="tc_bf16x2", device=local)
+            gb = torch.empty_like(xd)
+            for _ in range(3):
+                be.evaluate(xd, gb)
+            torch.cuda.synchronize()
+            bs = torch.cuda.ExternalStream(be.stream)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(bs)
+            for _ in range(args.compare_steps):
+                _lib.check(lib.ccm_evaluate_async(be.handle, xd.data_ptr(), gb.data_ptr(), xd.numel()))
+            b.record(bs)
+            b.synchronize()
+            bv = args.compare_steps / (a.elapsed_time(b) / 1e3)
+            be.evaluate(xd, gb)
+            f_b = be.result().fx
+            g_b = gb.cpu().numpy()
+            be.close()
+            other = {"evals_per_s": bv, "steps": args.compare_steps,
+                     "arithmetic": PATH_ARITHMETIC["tc_bf16x2"],
+                     "precision": None if args.no_precision
+                     else precision_block(msa, w, x, g_b, f_b, L)}
+
         plain = None
         if args.plain_steps > 0 and world == 1:
             pe = cb.Evaluator(msa, weights=w, path="simt_f32", device=local)
@@ -505,11 +552,12 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks,
             "plain_f32": plain,
+            "tc_bf16x2": other,
             "reference_cuda": ref_cuda,
             "precision": prec,
             "init_ms": {"weights": init_ms},
         }
-        print(json.dumps(out))
+        emit((out))
     barrier(world)
     if world > 1:
         import torch.distributed as dist

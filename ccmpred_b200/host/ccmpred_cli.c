@@ -158,6 +158,7 @@ int main(int argc, char **argv) {
 	o.lambda_pair = lambda_pair;
 	o.device = device;
 	const char *path = getenv("CCM_PATH");
+	if (path && strcmp(path, "tc_bf16x2") == 0) o.path = CCM_PATH_TC_BF16X2;
 	if (path && strcmp(path, "tc_bf16x3") == 0) o.path = CCM_PATH_TC_BF16X3;
 	if (path && strcmp(path, "simt_f32") == 0) o.path = CCM_PATH_SIMT_F32;
 	ccm_context *ctx = NULL;
