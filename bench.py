@@ -305,8 +305,14 @@ def reference_cuda_timing(msa, x, xd, steps, with_precision):
     return out
 
 
-def traffic_from_profiles(kernel: str):
-    path = os.path.join(ROOT, "profiles", "tc_kernels_L300_N5000.json")
+def traffic_from_profiles(kernel: str, path_name: str):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary
+    of the path's kernels (tc_* for the bf16 paths, i8_* for the integer path)."""
+    if path_name == "tc_i8x3":
+        fname, kernel = "i8_kernels_L300_N5000.json", kernel.replace("tc_", "i8_")
+    else:
+        fname = "tc_kernels_L300_N5000.json"
+    path = os.path.join(ROOT, "profiles", fname)
     if not os.path.exists(path):
         return None
     with open(path) as f:
@@ -456,7 +462,7 @@ def main():
         dom = max(("tc_forward", "tc_backward"), key=lambda k: kernels.get(k, 0.0))
         dom_ms = kernels.get(dom, float("nan"))
         achieved = flops / (dom_ms / 1e3) / 1e12
-        traffic = traffic_from_profiles(dom)
+        traffic = traffic_from_profiles(dom, args.path)
         # tensor-core flops actually issued by the dominant kernel: every split term,
         # the padded shapes (S = 256 slots per 12 columns, rows padded to 256) and,
         # for the backward, both products O^T R and R^T O on the upper-triangle tiles
