@@ -106,3 +106,66 @@ def test_tc_stages(gpu, path, L, N, seed):
     g1_exp = R_gpu[:, sl[:20].reshape(-1)].sum(axis=0).reshape(20, L)
     assert np.abs(g1d - g1_exp).max() <= 1e-5 * max(1.0, np.abs(g1_exp).max())
     ev.close()
+
+
+def digits_value(d0, d1, d2):
+    """Integer Q of the three stored bytes: d0 signed, d1 and d2 in 0..127."""
+    return d0.view(np.int8).astype(np.int64) * 16384 + d1.astype(np.int64) * 128 + d2.astype(np.int64)
+
+
+@pytest.mark.parametrize("L,N,seed", [(13, 50, 1), (24, 130, 2), (5, 7, 3)])
+def test_integer_path_stages(gpu, L, N, seed):
+    """The integer path: column maxima of |W| exactly, the three digits of every
+    W entry equal to clamp(rint(W * 2^(21 - e)), -2^21, 2^21 - 1) with e the
+    column's exponent (bit-exact integers), the one-hot bytes, and the digits of R
+    against an FP64 restatement of the forward at the quantised W (2^-21 abs)."""
+    import torch
+    msa = synth.generate(synth.MSAConfig("t", L, N, n_pairs=2, seed=seed))
+    w = np.random.default_rng(seed).uniform(0.2, 1.0, N).astype(np.float32)
+    x = synth.random_x(L, seed + 10, w_sd=0.05)
+    lam2 = 0.2 * (L - 1)
+    ev = Evaluator(msa, weights=w, lambda_pair=lam2, path="tc_i8x3")
+    xd = torch.from_numpy(x).cuda()
+    gd = torch.empty_like(xd)
+    ev.evaluate(xd, gd)
+    O, Wp, V, sl, S, Npad = expected_internals(msa, w, x, L, lam2)
+    nsp = 20 * L + 32 - (20 * L) % 32
+    W = x[nsp:].reshape(Q, L, QP, L)[:, :, :Q, :]                       # [b,k,a,j] float32
+
+    # column maxima over rows (b,k) of |W(b,k,a,j)|, per column c = a*L + j
+    cm = fetch(ev, 8, np.uint32).view(np.float32).reshape(Q, L)         # [a, j]
+    assert np.array_equal(cm, np.abs(W).max(axis=(0, 1)))
+    # exponent: smallest e with 2^e >= max (0 for an all-zero column)
+    mant, ex = np.frexp(cm.astype(np.float64))                          # cm = mant * 2^ex, mant in [0.5,1)
+    e = np.where(cm == 0, 0, np.where(mant == 0.5, ex - 1, ex))
+
+    # one-hot bytes (x1 copy)
+    O1 = fetch(ev, 0, np.uint8).reshape(Npad, S)
+    assert np.array_equal(O1, O.astype(np.uint8))
+
+    # digits of W in the slot layout, exact
+    d = [fetch(ev, 1 + i, np.uint8).reshape(S, S) for i in range(3)]
+    Qgpu = digits_value(*d)
+    Qexp = np.zeros((S, S), dtype=np.int64)
+    scale = np.ldexp(1.0, 21 - e)                                       # [a, j]
+    Wq = np.clip(np.rint(W.astype(np.float64) * scale[None, None]), -2**21, 2**21 - 1)
+    Qexp[np.ix_(sl.reshape(-1), sl.reshape(-1))] = Wq.astype(np.int64).reshape(Q * L, Q * L)
+    assert np.array_equal(Qgpu, Qexp)
+
+    # forward at the quantised W: logits, softmax, R = w (P - onehot); R digits at scale 1
+    Wdeq = np.zeros((S, S))
+    Wdeq[np.ix_(sl.reshape(-1), sl.reshape(-1))] = (Wq / scale[None, None]).reshape(Q * L, Q * L)
+    logits = O[:N] @ Wdeq
+    R_exp = np.zeros((Npad, S))
+    for l in range(L):
+        cols = sl[:, l]
+        z = logits[:, cols].copy()
+        z[:, :20] += V[:, l][None, :]
+        z -= z.max(axis=1, keepdims=True)
+        P = np.exp(z) / np.exp(z).sum(axis=1, keepdims=True)
+        onehot = (msa[:, l][:, None] == np.arange(Q)[None, :]).astype(np.float64)
+        R_exp[:N, cols] = w[:, None] * (P - onehot)
+    r = [fetch(ev, 4 + i, np.uint8).reshape(Npad, S) for i in range(3)]
+    R_gpu = digits_value(*r) / 2.0**21
+    assert np.abs(R_gpu - R_exp).max() < 2.0**-21 + 2e-6
+    ev.close()
