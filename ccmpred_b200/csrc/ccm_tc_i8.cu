@@ -330,7 +330,9 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
   }
   named_bar_sync(pair_bar, 64);
   double floss = 0.0;
-  float cf[kGroupCols];
+  // R * 2^21 = e * cw - [observed] * won, with cw = w exp(m - M) / S * 2^21
+  float cw[kGroupCols];
+  const float won = live ? wn * (float)(1 << kI8FracBits) : 0.0f;
 #pragma unroll
   for (int jj = 0; jj < kGroupCols; ++jj) {
     const float mo = other[jj], so = other[kGroupCols + jj];
@@ -338,7 +340,7 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
     const float fa = expf(mx[jj] - M), fo = expf(mo - M);
     const float S = H == 0 ? se[jj] * fa + so * fo : so * fo + se[jj] * fa;
     const float lse = M + logf(S);
-    cf[jj] = fa / S;
+    cw[jj] = xr[jj] >= 0 ? (fa / S) * won : 0.0f;
     if (xr[jj] >= 0 && ((xr[jj] * kGroupCols + jj) >> 7) == H)
       floss += (double)(wn * (lse - tg[jj]));
   }
@@ -355,24 +357,27 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
     uint32_t w0[8], w1[8], w2[8];
 #pragma unroll
     for (int e4 = 0; e4 < 8; ++e4) {
-      uint32_t h0 = 0, h1 = 0, h2 = 0;
+      int qv[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int i = e4 * 4 + e;
         const int col = cc * 32 + i;
-        float r = 0.0f;
+        float t = 0.0f;
         if (col < kGroupUsed) {
           const int a = col / kGroupCols, jj = col % kGroupCols;
-          if (xr[jj] >= 0)
-            r = wn * (__uint_as_float(v[i]) * cf[jj] - (xr[jj] == a ? 1.0f : 0.0f));
+          t = fmaf(__uint_as_float(v[i]), cw[jj], xr[jj] == a ? -won : 0.0f);
         }
-        uint32_t d0, d1, d2;
-        digits_of(r, (float)(1 << kI8FracBits), d0, d1, d2);
-        h0 |= d0 << (8 * e);
-        h1 |= d1 << (8 * e);
-        h2 |= d2 << (8 * e);
+        // |R| < 1: only the top of the range needs the clamp (P rounding to 1)
+        qv[e] = min(__float2int_rn(t), (1 << kI8FracBits) - 1);
       }
-      w0[e4] = h0; w1[e4] = h1; w2[e4] = h2;
+      // byte e of each word = digit of element e: d0 = q >> 14, d1 = (q >> 7) & 127,
+      // d2 = q & 127 (two byte permutes per pair, one per word)
+      auto pack = [](int b0, int b1, int b2, int b3) {
+        return __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
+      };
+      w0[e4] = pack(qv[0] >> 14, qv[1] >> 14, qv[2] >> 14, qv[3] >> 14);
+      w1[e4] = pack(qv[0] >> 7, qv[1] >> 7, qv[2] >> 7, qv[3] >> 7) & 0x7F7F7F7Fu;
+      w2[e4] = pack(qv[0], qv[1], qv[2], qv[3]) & 0x7F7F7F7Fu;
     }
     const long long off = rbase + cc * 32;
     st_global_v8(args.r[0] + off, w0);
