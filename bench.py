@@ -357,7 +357,7 @@ def run_batch(args, world, rank, local):
     emit(({
         "metric": "MSAs/s, 256 ragged alignments solved to convergence", "value": value,
         "unit": "MSAs/s", "n_gpus": world, "higher_is_better": True, "scaling": "weak",
-        "data": "synthetic", "dtype": "bf16",
+        "data": "synthetic", "dtype": "int8",
         "config": {"workload": "batch256: L~U[50,400], N~logU[200,20000], seeds 1000+i, "
                                "eps 1e-3 or 250 iterations",
                    "workers": args.batch_workers, "path": "tc_i8x3"},

@@ -54,16 +54,6 @@ __device__ __forceinline__ int col_exponent(uint32_t mbits) {
   return max(e, -100);
 }
 
-// The three digits of v at scale 2^e, given scale_in = 2^(21 - e).
-__device__ __forceinline__ void digits_of(float v, float scale_in, uint32_t &d0, uint32_t &d1,
-                                          uint32_t &d2) {
-  int q = __float2int_rn(v * scale_in);  // exact scaling by a power of two, one rounding
-  q = min(max(q, -(1 << kI8FracBits)), (1 << kI8FracBits) - 1);
-  d0 = (uint32_t)(q >> 14) & 0xFFu;
-  d1 = (uint32_t)(q >> 7) & 127u;
-  d2 = (uint32_t)q & 127u;
-}
-
 // ---------------------------------------------------------------- colmax
 // Column maxima of |W| over the 21 L rows (b, k), per coupling column c = a*L + j
 // (a < 21), as float bits with atomicMax (|v| >= 0 orders like its bits).  Block
@@ -103,6 +93,14 @@ __global__ void __launch_bounds__(256) i8_colmax_kernel(const float *__restrict_
   if (c < kQ * L && m > 0.0f) atomicMax(colmax + c, __float_as_uint(m));
 }
 
+// Per coupling column c: the encoding factor 2^(21 - e) of its digits, e the
+// column's exponent (from the maxima above); one value per column, read by prep.
+__global__ void i8_scales_kernel(const uint32_t *__restrict__ colmax, float *__restrict__ enc,
+                                 int ncols) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < ncols) enc[c] = pow2f(kI8FracBits - col_exponent(colmax[c]));
+}
+
 // ---------------------------------------------------------------- prep
 // One block per row (b, k) of W, as tc_prep: g2 <- g2_coef * lambda2 * x, the FP64
 // partial of sum x^2, and row s(b, k) of the three digit matrices of Wperm (16
@@ -133,8 +131,9 @@ __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ 
       for (int u = 0; u < kU; ++u) {
         const int i = i0 + u * blockDim.x;
         if (i < n4) {
-          acc += (double)v[u].x * v[u].x + (double)v[u].y * v[u].y + (double)v[u].z * v[u].z +
-                 (double)v[u].w * v[u].w;
+          // four squares in float, their sum added in FP64
+          acc += (double)fmaf(v[u].w, v[u].w,
+                              fmaf(v[u].z, v[u].z, fmaf(v[u].y, v[u].y, v[u].x * v[u].x)));
           if (i < nreal4) reinterpret_cast<float4 *>(xrow)[i] = v[u];
           __stcs(dst + i, make_float4(two_l2 * v[u].x, two_l2 * v[u].y, two_l2 * v[u].z,
                                       two_l2 * v[u].w));
@@ -155,25 +154,29 @@ __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ 
     uint32_t p0[4], p1[4], p2[4];
 #pragma unroll
     for (int e4 = 0; e4 < 4; ++e4) {
-      uint32_t h0 = 0, h1 = 0, h2 = 0;
+      int qv[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int sl = u * 16 + e4 * 4 + e;
         const int t = sl / kGroupSlots, r = sl % kGroupSlots;
-        uint32_t d0 = 0, d1 = 0, d2 = 0;
+        int q = 0;
         if (r < kGroupUsed) {
           const int a = r / kGroupCols, j = t * kGroupCols + r % kGroupCols;
           if (j < L) {
             const int c = a * L + j;
-            digits_of(xrow[c], pow2f(kI8FracBits - col_exponent(__ldg(args.colmax + c))), d0,
-                      d1, d2);
+            q = __float2int_rn(xrow[c] * __ldg(args.enc + c));  // exact power-of-two scaling
+            q = min(max(q, -(1 << kI8FracBits)), (1 << kI8FracBits) - 1);
           }
         }
-        h0 |= d0 << (8 * e);
-        h1 |= d1 << (8 * e);
-        h2 |= d2 << (8 * e);
+        qv[e] = q;
       }
-      p0[e4] = h0; p1[e4] = h1; p2[e4] = h2;
+      // byte e of each word = digit of element e (as in the forward's R digits)
+      auto pack = [](int b0, int b1, int b2, int b3) {
+        return __byte_perm(__byte_perm(b0, b1, 0x0040), __byte_perm(b2, b3, 0x0040), 0x5410);
+      };
+      p0[e4] = pack(qv[0] >> 14, qv[1] >> 14, qv[2] >> 14, qv[3] >> 14);
+      p1[e4] = pack(qv[0] >> 7, qv[1] >> 7, qv[2] >> 7, qv[3] >> 7) & 0x7F7F7F7Fu;
+      p2[e4] = pack(qv[0], qv[1], qv[2], qv[3]) & 0x7F7F7F7Fu;
     }
     const long long off = srow + (long long)u * 16;
     *reinterpret_cast<uint4 *>(args.wdig[0] + off) = make_uint4(p0[0], p0[1], p0[2], p0[3]);
@@ -889,9 +892,12 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   else
     i8_colmax_kernel<false><<<cgrid, 256, 0, c->stream>>>(d_x, nullptr, nullptr, nullptr,
                                                            c->d_colmax, L, c->nsp, kRows);
+  float *enc = reinterpret_cast<float *>(c->d_colmax + kQ * L);
+  i8_scales_kernel<<<(kQ * L + 255) / 256, 256, 0, c->stream>>>(c->d_colmax, enc, kQ * L);
   I8PrepArgs pa{};
   for (int i = 0; i < 3; ++i) pa.wdig[i] = c->d_wdig[i];
   pa.colmax = c->d_colmax;
+  pa.enc = enc;
   pa.part_reg = c->d_part_reg;
   pa.L = L; pa.S = c->S; pa.lambda_pair = c->lambda_pair;
   pa.g2_coef = c->gradient == CCM_GRADIENT_PARTIAL ? 1.0f : 2.0f;
@@ -924,7 +930,7 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
 
   launch_tc_finalize(c, x1, d_g, 2LL * pair_tiles);
   prof_mark(c);
-  count_launch(c, 5);
+  count_launch(c, 6);
   return cudaGetLastError();
 }
 
