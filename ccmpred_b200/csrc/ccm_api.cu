@@ -220,7 +220,7 @@ int alloc_tc(ccm_context *c) {
       CCM_CUDA_TRY(dev_alloc(c, &c->d_rdig[i], Np * S));
       CCM_CUDA_TRY(cudaMemsetAsync(c->d_rdig[i], 0, Np * S, c->stream));
     }
-    CCM_CUDA_TRY(dev_alloc(c, &c->d_colmax, 2 * sizeof(uint32_t) * kQ * c->L));
+    CCM_CUDA_TRY(dev_alloc(c, &c->d_colmax, sizeof(uint32_t) * (((kQ * c->L + 3) & ~3) + S)));
   } else {
     CCM_CUDA_TRY(dev_alloc(c, &c->d_onehot, sizeof(__nv_bfloat16) * Np * S));
     for (int i = 0; i < c->nsplit; ++i) {

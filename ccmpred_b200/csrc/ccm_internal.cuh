@@ -38,9 +38,10 @@ struct I8BwdMaps {
 struct I8PrepArgs {
   int8_t *wdig[3];
   const uint32_t *colmax;  // per coupling column (a*L + j): max |W| as float bits
-  const float *enc;        // per coupling column: the digit encoding factor 2^(21 - e)
+  const float *enc;        // per slot: the digit encoding factor 2^(21 - e), 0 for padding
   double *part_reg;
   int L, S;
+  float inv_L;
   float lambda_pair;
   float g2_coef;
 };
@@ -201,7 +202,7 @@ struct ccm_context {
   uint8_t *d_o1 = nullptr, *d_o128 = nullptr;          // Npad x S one-hot, values 1 / 128
   int8_t *d_wdig[3] = {nullptr, nullptr, nullptr};     // S x S digits of W
   int8_t *d_rdig[3] = {nullptr, nullptr, nullptr};     // Npad x S digits of R
-  uint32_t *d_colmax = nullptr;  // 21 L column maxima of |W|, then 21 L encoding factors
+  uint32_t *d_colmax = nullptr;  // 21 L column maxima of |W|, then S per-slot encoding factors
   ccm::I8FwdMaps i8fwd_maps;
   ccm::I8BwdMaps i8bwd_maps;
 

@@ -93,21 +93,30 @@ __global__ void __launch_bounds__(256) i8_colmax_kernel(const float *__restrict_
   if (c < kQ * L && m > 0.0f) atomicMax(colmax + c, __float_as_uint(m));
 }
 
-// Per coupling column c: the encoding factor 2^(21 - e) of its digits, e the
-// column's exponent (from the maxima above); one value per column, read by prep.
+// Per slot s: the encoding factor 2^(21 - e) of the digits of its coupling column
+// (e the column's exponent, from the maxima above), 0 for padding slots; read by prep.
 __global__ void i8_scales_kernel(const uint32_t *__restrict__ colmax, float *__restrict__ enc,
-                                 int ncols) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < ncols) enc[c] = pow2f(kI8FracBits - col_exponent(colmax[c]));
+                                 int L, int S) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S) return;
+  const int t = s / kGroupSlots, r = s % kGroupSlots;
+  float f = 0.0f;
+  if (r < kGroupUsed) {
+    const int a = r / kGroupCols, j = t * kGroupCols + r % kGroupCols;
+    if (j < L) f = pow2f(kI8FracBits - col_exponent(colmax[a * L + j]));
+  }
+  enc[s] = f;
 }
 
 // ---------------------------------------------------------------- prep
 // One block per row (b, k) of W, as tc_prep: g2 <- g2_coef * lambda2 * x, the FP64
 // partial of sum x^2, and row s(b, k) of the three digit matrices of Wperm (16
-// slots per thread, one 16-byte store per digit matrix).
+// slots per thread, one 16-byte store per digit matrix).  The row is staged in
+// shared memory in slot order, so that the digit pass reads 16 consecutive slots
+// per thread (vector loads, no index arithmetic) with their per-slot factors.
 __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ x2,
                                                       float *__restrict__ g2, I8PrepArgs args) {
-  extern __shared__ __align__(16) float xrow[];  // 21 L floats
+  extern __shared__ __align__(16) float xrow[];  // S floats: the row in slot order
   const int L = args.L;
   const int row = blockIdx.x;
   const int b = row / L, k = row % L;
@@ -134,7 +143,16 @@ __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ 
           // four squares in float, their sum added in FP64
           acc += (double)fmaf(v[u].w, v[u].w,
                               fmaf(v[u].z, v[u].z, fmaf(v[u].y, v[u].y, v[u].x * v[u].x)));
-          if (i < nreal4) reinterpret_cast<float4 *>(xrow)[i] = v[u];
+          if (i < nreal4) {
+            // c = 4i = a L + j, j a multiple of 4: the four elements share a, and
+            // j .. j+3 stay inside the row's column range
+            const int c = 4 * i;
+            const int a = (int)(((float)c + 0.5f) * args.inv_L);
+            const int j = c - a * L;
+            const float vv[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) xrow[slot_of(a, j + e)] = vv[e];
+          }
           __stcs(dst + i, make_float4(two_l2 * v[u].x, two_l2 * v[u].y, two_l2 * v[u].z,
                                       two_l2 * v[u].w));
         }
@@ -144,7 +162,7 @@ __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ 
     for (int i = threadIdx.x; i < kQPad * L; i += blockDim.x) {
       const float v = x2[base + i];
       acc += (double)v * v;
-      if (i < nreal) xrow[i] = v;
+      if (i < nreal) xrow[slot_of(i / L, i % L)] = v;
       g2[base + i] = two_l2 * v;
     }
   }
@@ -154,21 +172,15 @@ __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ 
     uint32_t p0[4], p1[4], p2[4];
 #pragma unroll
     for (int e4 = 0; e4 < 4; ++e4) {
+      const float4 xv = reinterpret_cast<const float4 *>(xrow)[u * 4 + e4];
+      const float4 fv = __ldg(reinterpret_cast<const float4 *>(args.enc) + u * 4 + e4);
+      const float xs[4] = {xv.x, xv.y, xv.z, xv.w}, fs[4] = {fv.x, fv.y, fv.z, fv.w};
       int qv[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        const int sl = u * 16 + e4 * 4 + e;
-        const int t = sl / kGroupSlots, r = sl % kGroupSlots;
-        int q = 0;
-        if (r < kGroupUsed) {
-          const int a = r / kGroupCols, j = t * kGroupCols + r % kGroupCols;
-          if (j < L) {
-            const int c = a * L + j;
-            q = __float2int_rn(xrow[c] * __ldg(args.enc + c));  // exact power-of-two scaling
-            q = min(max(q, -(1 << kI8FracBits)), (1 << kI8FracBits) - 1);
-          }
-        }
-        qv[e] = q;
+        // padding slots have factor 0 and are never staged: their digits are 0
+        const int q = fs[e] != 0.0f ? __float2int_rn(xs[e] * fs[e]) : 0;  // exact scaling
+        qv[e] = min(max(q, -(1 << kI8FracBits)), (1 << kI8FracBits) - 1);
       }
       // byte e of each word = digit of element e (as in the forward's R digits)
       auto pack = [](int b0, int b1, int b2, int b3) {
@@ -892,8 +904,9 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   else
     i8_colmax_kernel<false><<<cgrid, 256, 0, c->stream>>>(d_x, nullptr, nullptr, nullptr,
                                                            c->d_colmax, L, c->nsp, kRows);
-  float *enc = reinterpret_cast<float *>(c->d_colmax + kQ * L);
-  i8_scales_kernel<<<(kQ * L + 255) / 256, 256, 0, c->stream>>>(c->d_colmax, enc, kQ * L);
+  // per-slot factors after the column maxima, 16-byte aligned for the float4 loads
+  float *enc = reinterpret_cast<float *>(c->d_colmax + ((kQ * L + 3) & ~3));
+  i8_scales_kernel<<<(c->S + 255) / 256, 256, 0, c->stream>>>(c->d_colmax, enc, L, c->S);
   I8PrepArgs pa{};
   for (int i = 0; i < 3; ++i) pa.wdig[i] = c->d_wdig[i];
   pa.colmax = c->d_colmax;
@@ -901,7 +914,8 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   pa.part_reg = c->d_part_reg;
   pa.L = L; pa.S = c->S; pa.lambda_pair = c->lambda_pair;
   pa.g2_coef = c->gradient == CCM_GRADIENT_PARTIAL ? 1.0f : 2.0f;
-  i8_prep_kernel<<<kQ * L, 256, sizeof(float) * kQ * L, c->stream>>>(x2, g2, pa);
+  pa.inv_L = 1.0f / (float)L;
+  i8_prep_kernel<<<kQ * L, 256, sizeof(float) * c->S, c->stream>>>(x2, g2, pa);
   prof_mark(c);
 
   I8FwdArgs fa{};
@@ -936,8 +950,10 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
 
 cudaError_t i8_configure_kernels() {
   cudaError_t e;
+  // the staged row is S floats: up to L = 2688 (the 227 KB per block, less the
+  // kernel's static reduction buffer)
   if ((e = cudaFuncSetAttribute(i8_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                168000)) != cudaSuccess)
+                                230000)) != cudaSuccess)
     return e;
   if ((e = cudaFuncSetAttribute(i8_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 I8FwdSmem::kTotal)) != cudaSuccess)
