@@ -801,7 +801,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
             const long long qs = (long long)(int)vh[i] * 16384 + (long long)(int)vl[i];
-            accv[c * 16 + i] += (float)((double)qs * 4.76837158203125e-07);  // 2^-21
+            // exact 64-bit sum, one rounding to float, exact scaling by 2^-21
+            accv[c * 16 + i] += __ll2float_rn(qs) * 4.76837158203125e-07f;
           }
         }
         tc_fence_before();
