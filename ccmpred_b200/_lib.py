@@ -24,8 +24,10 @@ PATH_TC_BF16X3 = 1
 PATH_SIMT_F32 = 2
 PATH_SIMT_F64 = 3
 PATH_TC_I8X3 = 4
+PATH_TC_I8SP = 5
 PATHS = {"tc_bf16x2": PATH_TC_BF16X2, "tc_bf16x3": PATH_TC_BF16X3,
-         "simt_f32": PATH_SIMT_F32, "simt_f64": PATH_SIMT_F64, "tc_i8x3": PATH_TC_I8X3}
+         "simt_f32": PATH_SIMT_F32, "simt_f64": PATH_SIMT_F64, "tc_i8x3": PATH_TC_I8X3,
+         "tc_i8sp": PATH_TC_I8SP}
 
 
 GRADIENT_TIED = 0

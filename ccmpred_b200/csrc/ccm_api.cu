@@ -143,10 +143,13 @@ int make_map_bf16(CUtensorMap *map, void *base, long long rows, long long cols, 
 
 // 2-D 8-bit row-major [rows][cols] tensor, boxes of box_cols x box_rows bytes
 // (128-byte swizzle for 128-column boxes, 64-byte swizzle for 64-column boxes).
+// 8-bit row-major [rows][cols] map; the swizzle spans the box's 128 or 64 bytes
+// unless given.
 int make_map_u8(CUtensorMap *map, void *base, long long rows, long long cols, int box_cols,
-                int box_rows) {
+                int box_rows, int swizzle = -1) {
   const CUtensorMapSwizzle swz =
-      box_cols == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
+      swizzle >= 0 ? (CUtensorMapSwizzle)swizzle
+                   : (box_cols == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B);
   EncodeTiledFn enc = get_encode_fn();
   if (!enc) return set_error(CCM_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
   cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
@@ -204,21 +207,38 @@ int ensure_configured(int device) {
 }
 
 int alloc_tc(ccm_context *c) {
-  c->T = n_groups(c->L);
-  c->S = c->T * kGroupSlots;
+  const bool sp = c->path == CCM_PATH_TC_I8SP;
+  if (sp) {
+    // sparse integer path: forward tiles are 192-slot groups (9 columns); the
+    // slot space is padded to the backward's 256-slot pair tiles; K of the
+    // forward is 21 L in the order l * 21 + q, padded to 256
+    c->T = Groups192::groups(c->L);
+    c->SW = c->T * Groups192::kSlots;
+    c->S = ((c->SW + 255) / 256) * 256;
+    c->KP = ((kQ * c->L + 255) / 256) * 256;
+  } else {
+    c->T = n_groups(c->L);
+    c->S = c->T * kGroupSlots;
+  }
   // rows padded to the forward's 256-row CTA-pair tiles
   c->Npad = ((c->N + 255) / 256) * 256;
   const size_t S = c->S, Np = c->Npad;
-  const bool i8 = c->path == CCM_PATH_TC_I8X3;
+  const bool i8 = c->path == CCM_PATH_TC_I8X3 || sp;
   if (i8) {
     // integer path: one-hot x1 / x128 bytes, three digit matrices of W and of R
+    const size_t wbytes = sp ? (size_t)c->KP * c->SW : S * S;
     CCM_CUDA_TRY(dev_alloc(c, &c->d_o1, Np * S));
     CCM_CUDA_TRY(dev_alloc(c, &c->d_o128, Np * S));
     for (int i = 0; i < 3; ++i) {
-      CCM_CUDA_TRY(dev_alloc(c, &c->d_wdig[i], S * S));
-      CCM_CUDA_TRY(cudaMemsetAsync(c->d_wdig[i], 0, S * S, c->stream));
+      CCM_CUDA_TRY(dev_alloc(c, &c->d_wdig[i], wbytes));
+      CCM_CUDA_TRY(cudaMemsetAsync(c->d_wdig[i], 0, wbytes, c->stream));
       CCM_CUDA_TRY(dev_alloc(c, &c->d_rdig[i], Np * S));
       CCM_CUDA_TRY(cudaMemsetAsync(c->d_rdig[i], 0, Np * S, c->stream));
+    }
+    if (sp) {
+      CCM_CUDA_TRY(dev_alloc(c, &c->d_ac1, Np * c->KP / 2));
+      CCM_CUDA_TRY(dev_alloc(c, &c->d_ac128, Np * c->KP / 2));
+      CCM_CUDA_TRY(dev_alloc(c, &c->d_meta, Np * c->KP / 8));
     }
     CCM_CUDA_TRY(dev_alloc(c, &c->d_colmax, sizeof(uint32_t) * (((kQ * c->L + 3) & ~3) + S)));
   } else {
@@ -238,8 +258,9 @@ int alloc_tc(ccm_context *c) {
   std::vector<int2> tiles;
   // P and Q in 256-slot blocks (rows, columns of C); the symmetric gradient
   // needs only the tiles that hold some s1 <= s2
-  for (int Q = 0; Q < c->T; ++Q)
-    for (int P = 0; P < c->T; ++P)
+  const int blocks = c->S / 256;
+  for (int Q = 0; Q < blocks; ++Q)
+    for (int P = 0; P < blocks; ++P)
       if (c->gradient == CCM_GRADIENT_PARTIAL || P <= Q) tiles.push_back(make_int2(P, Q));
   c->n_bwd_tiles = (int)tiles.size();
   CCM_CUDA_TRY(dev_alloc(c, &c->d_bwd_tiles, sizeof(int2) * tiles.size()));
@@ -256,8 +277,26 @@ int alloc_tc(ccm_context *c) {
     if ((rc = make_map_u8(&c->i8bwd_maps.o1, c->d_o1, Np, S, 128, 32)) != CCM_OK) return rc;
     if ((rc = make_map_u8(&c->i8bwd_maps.o128, c->d_o128, Np, S, 128, 32)) != CCM_OK) return rc;
     for (int i = 0; i < 3; ++i) {
-      if ((rc = make_map_u8(&c->i8fwd_maps.b[i], c->d_wdig[i], S, S, 128, 64)) != CCM_OK) return rc;
+      if (!sp && (rc = make_map_u8(&c->i8fwd_maps.b[i], c->d_wdig[i], S, S, 128, 64)) != CCM_OK)
+        return rc;
       if ((rc = make_map_u8(&c->i8bwd_maps.r[i], c->d_rdig[i], Np, S, 128, 32)) != CCM_OK) return rc;
+    }
+    if (sp) {
+      std::memset(&c->i8sp_maps, 0, sizeof(c->i8sp_maps));
+      // tiled operand storage viewed as rows of 256 bytes; one box = one stage tile
+      const long long KP = c->KP;
+      const int none = CU_TENSOR_MAP_SWIZZLE_NONE;
+      if ((rc = make_map_u8(&c->i8sp_maps.a1, c->d_ac1, Np * KP / 512, 256, 256, 32, none)) !=
+              CCM_OK ||
+          (rc = make_map_u8(&c->i8sp_maps.a128, c->d_ac128, Np * KP / 512, 256, 256, 32, none)) !=
+              CCM_OK ||
+          (rc = make_map_u8(&c->i8sp_maps.e, c->d_meta, Np * KP / 2048, 256, 256, 8, none)) !=
+              CCM_OK)
+        return rc;
+      for (int i = 0; i < 3; ++i)
+        if ((rc = make_map_u8(&c->i8sp_maps.b[i], c->d_wdig[i], KP * c->SW / 256, 256, 256, 48,
+                              none)) != CCM_OK)
+          return rc;
     }
     return CCM_OK;
   }
@@ -291,7 +330,7 @@ void free_all(ccm_context *c) {
   auto f = [c](void *p) { if (p) cudaFreeAsync(p, c->stream); };
   f(c->d_msa); f(c->d_w); f(c->d_out); f(c->d_onehot);
   for (int i = 0; i < 3; ++i) { f(c->d_wperm[i]); f(c->d_r[i]); f(c->d_wdig[i]); f(c->d_rdig[i]); }
-  f(c->d_o1); f(c->d_o128); f(c->d_colmax);
+  f(c->d_o1); f(c->d_o128); f(c->d_colmax); f(c->d_ac1); f(c->d_ac128); f(c->d_meta);
   f(c->d_part_f); f(c->d_part_reg); f(c->d_g1d); f(c->d_bwd_tiles);
   f(c->d_simt_pc); f(c->d_simt_g2); f(c->d_simt_part); f(c->d_simt_g1);
   f(c->d_xh); f(c->d_gh);
@@ -319,7 +358,8 @@ int enqueue_eval(ccm_context *c, const float *d_x, float *d_g) {
   switch (c->path) {
     case CCM_PATH_TC_BF16X2:
     case CCM_PATH_TC_BF16X3: e = tc_evaluate(c, d_x, d_g); break;
-    case CCM_PATH_TC_I8X3: e = i8_evaluate(c, d_x, d_g, nullptr, nullptr, nullptr); break;
+    case CCM_PATH_TC_I8X3:
+    case CCM_PATH_TC_I8SP: e = i8_evaluate(c, d_x, d_g, nullptr, nullptr, nullptr); break;
     case CCM_PATH_SIMT_F32: e = simt_evaluate(c, d_x, d_g); break;
     case CCM_PATH_SIMT_F64:
       return set_error(CCM_ERR_INVALID, "CCM_PATH_SIMT_F64 takes double buffers: use ccm_evaluate_f64");
@@ -348,12 +388,12 @@ void free_prof(ccm_context *c) {
 
 int ccm::enqueue_evaluation_step(ccm_context *c, const float *d_x, const float *d_s,
                                   const double *d_alpha, float *d_xt, float *d_g) {
-  if (c->path != CCM_PATH_TC_BF16X2 && c->path != CCM_PATH_TC_BF16X3 &&
-      c->path != CCM_PATH_TC_I8X3)
+  const bool i8 = c->path == CCM_PATH_TC_I8X3 || c->path == CCM_PATH_TC_I8SP;
+  if (c->path != CCM_PATH_TC_BF16X2 && c->path != CCM_PATH_TC_BF16X3 && !i8)
     return set_error(CCM_ERR_INVALID, "fused step: tensor-core paths only");
   CCM_CUDA_TRY(cudaMemsetAsync(c->d_out, 0, sizeof(ccm_result), c->stream));
   c->prof_idx = 0;
-  const cudaError_t e = c->path == CCM_PATH_TC_I8X3
+  const cudaError_t e = i8
                             ? i8_evaluate(c, d_x, d_g, d_s, d_alpha, d_xt)
                             : tc_evaluate_step(c, d_x, d_s, d_alpha, d_xt, d_g);
   if (e != cudaSuccess)
@@ -420,7 +460,7 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
   *out = nullptr;
   ccm_options o;
   if (opt) o = *opt; else ccm_options_default(&o, ncol);
-  if (o.path < CCM_PATH_TC_BF16X2 || o.path > CCM_PATH_TC_I8X3)
+  if (o.path < CCM_PATH_TC_BF16X2 || o.path > CCM_PATH_TC_I8SP)
     return set_error(CCM_ERR_INVALID, "ccm_create: unknown path %d", o.path);
   if (o.gradient != CCM_GRADIENT_TIED && o.gradient != CCM_GRADIENT_PARTIAL)
     return set_error(CCM_ERR_INVALID, "ccm_create: unknown gradient mode %d", o.gradient);
@@ -434,7 +474,7 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
   cudaDeviceProp prop;
   CCM_CUDA_TRY(cudaGetDeviceProperties(&prop, o.device));
   const bool tc_path = o.path == CCM_PATH_TC_BF16X2 || o.path == CCM_PATH_TC_BF16X3 ||
-                       o.path == CCM_PATH_TC_I8X3;
+                       o.path == CCM_PATH_TC_I8X3 || o.path == CCM_PATH_TC_I8SP;
   if (tc_path && prop.major != 10)
     return set_error(CCM_ERR_UNSUPPORTED, "tensor-core path needs an sm_100 device (found sm_%d%d)",
                      prop.major, prop.minor);
@@ -447,11 +487,12 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
   c->num_sms = prop.multiProcessorCount;
   if (tc_path) {
     const int ns = o.path == CCM_PATH_TC_BF16X3 ? 3 : 2;
-    cudaError_t e = o.path == CCM_PATH_TC_I8X3 ? i8_forward_max_pairs(&c->fwd_pairs)
+    const bool i8 = o.path == CCM_PATH_TC_I8X3 || o.path == CCM_PATH_TC_I8SP;
+    cudaError_t e = o.path == CCM_PATH_TC_I8SP ? i8sp_forward_max_pairs(&c->fwd_pairs)
+                    : i8                       ? i8_forward_max_pairs(&c->fwd_pairs)
                                                : tc_forward_max_pairs(ns, &c->fwd_pairs);
     if (e == cudaSuccess)
-      e = o.path == CCM_PATH_TC_I8X3 ? i8_backward_max_pairs(&c->bwd_pairs)
-                                     : tc_backward_max_pairs(ns, &c->bwd_pairs);
+      e = i8 ? i8_backward_max_pairs(&c->bwd_pairs) : tc_backward_max_pairs(ns, &c->bwd_pairs);
     if (e != cudaSuccess || c->fwd_pairs < 1 || c->bwd_pairs < 1) {
       delete c;
       return set_error(CCM_ERR_CUDA, "tc_forward cluster occupancy: %s", cudaGetErrorString(e));
@@ -604,11 +645,19 @@ long long ccm_debug_copy(ccm_context *c, int which, void *dst, long long bytes) 
   const void *src = nullptr;
   long long size = 0;
   const long long slots = (long long)c->S;
-  if (c->path == CCM_PATH_TC_I8X3) {
-    // integer path: 0 one-hot (x1 bytes), 1-3 digits of W, 4-6 digits of R,
-    // 7 single-field data gradient, 8 column maxima of |W| (float bits)
+  if (c->path == CCM_PATH_TC_I8X3 || c->path == CCM_PATH_TC_I8SP) {
+    // integer paths: 0 one-hot (x1 bytes), 1-3 digits of W, 4-6 digits of R,
+    // 7 single-field data gradient, 8 column maxima of |W| (float bits); sparse
+    // path: W digits are KP x SW, 9 compressed one-hot x1 (Npad x KP/2),
+    // 10 its metadata (Npad x KP/8)
+    const bool sp = c->path == CCM_PATH_TC_I8SP;
     if (which == 0) { src = c->d_o1; size = (long long)c->Npad * slots; }
-    else if (which >= 1 && which <= 3) { src = c->d_wdig[which - 1]; size = slots * slots; }
+    else if (which >= 1 && which <= 3) {
+      src = c->d_wdig[which - 1];
+      size = sp ? (long long)c->KP * c->SW : slots * slots;
+    }
+    else if (which == 9 && sp) { src = c->d_ac1; size = (long long)c->Npad * c->KP / 2; }
+    else if (which == 10 && sp) { src = c->d_meta; size = (long long)c->Npad * c->KP / 8; }
     else if (which >= 4 && which <= 6) { src = c->d_rdig[which - 4]; size = (long long)c->Npad * slots; }
     else if (which == 7) { src = c->d_g1d; size = 4LL * (kQ - 1) * c->L; }
     else if (which == 8) { src = c->d_colmax; size = 4LL * kQ * c->L; }

@@ -215,7 +215,7 @@ int capture_trial(CgState &st, int p) {
   // tensor-core paths take the step inside tc_prep (one pass over x and s that
   // also splits the couplings into the bf16 terms); the CUDA-core paths step first
   const bool fused = st.c->path == CCM_PATH_TC_BF16X2 || st.c->path == CCM_PATH_TC_BF16X3 ||
-                     st.c->path == CCM_PATH_TC_I8X3;
+                     st.c->path == CCM_PATH_TC_I8X3 || st.c->path == CCM_PATH_TC_I8SP;
   if (!fused) cg_step_kernel<<<grid_for(st.n), 256, 0, s>>>(x, st.s, st.d_alpha, xt, st.n);
   const long long before = st.c->launches;
   int rc = fused ? enqueue_evaluation_step(st.c, x, st.s, st.d_alpha, xt, gt)

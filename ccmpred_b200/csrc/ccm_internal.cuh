@@ -35,12 +35,23 @@ struct I8BwdMaps {
   CUtensorMap r[3];      // digits of R [Npad][S] s8, same box
 };
 
+// Sparse integer forward (CCM_PATH_TC_I8SP): compressed one-hot A and its
+// metadata, K in the order k' = l * 21 + q.
+// All four are tiled stores of shared-memory images (see ccm_tc_i8.cu) viewed
+// as rows of 256 bytes, no TMA swizzle; one box is one tile of one stage.
+struct I8SpMaps {
+  CUtensorMap a1, a128;  // compressed one-hot x1 / x128: 8 KB tiles, box 256 x 32
+  CUtensorMap e;         // metadata: 2 KB tiles, box 256 x 8
+  CUtensorMap b[3];      // digits of W: 12 KB tiles (128 K rows x 96 slots), box 256 x 48
+};
+
 struct I8PrepArgs {
   int8_t *wdig[3];
   const uint32_t *colmax;  // per coupling column (a*L + j): max |W| as float bits
   const float *enc;        // per slot: the digit encoding factor 2^(21 - e), 0 for padding
   double *part_reg;
   int L, S;
+  int KB;  // sparse forward: K blocks of 128 rows (tiled digit layout)
   float inv_L;
   float lambda_pair;
   float g2_coef;
@@ -55,6 +66,7 @@ struct I8FwdArgs {
   double *part_f;
   int *status;
   int L, N, S, T, Npad, m_tiles;
+  int KP;  // sparse forward: logical K (a multiple of 256)
 };
 
 struct PrepArgs {
@@ -135,6 +147,7 @@ cudaError_t i8_configure_kernels();
 cudaError_t i8_forward_max_pairs(int *pairs);
 cudaError_t i8_backward_max_pairs(int *pairs);
 cudaError_t i8_build_onehot(ccm_context *c);
+cudaError_t i8sp_forward_max_pairs(int *pairs);
 // tc_finalize over the loss partials of n_fwd_tiles 128-row forward tiles.
 cudaError_t launch_tc_finalize(ccm_context *c, const float *x1, float *d_g, long long n_fwd_tiles);
 // One CG trial on a tensor-core context: xt = x + alpha s (alpha on the device),
@@ -205,6 +218,11 @@ struct ccm_context {
   uint32_t *d_colmax = nullptr;  // 21 L column maxima of |W|, then S per-slot encoding factors
   ccm::I8FwdMaps i8fwd_maps;
   ccm::I8BwdMaps i8bwd_maps;
+  // sparse integer forward: W digits are KP x SW (K rows l * 21 + q, 192-slot
+  // groups as columns); compressed one-hot Npad x KP/2 and metadata Npad x KP/8
+  int KP = 0, SW = 0;
+  uint8_t *d_ac1 = nullptr, *d_ac128 = nullptr, *d_meta = nullptr;
+  ccm::I8SpMaps i8sp_maps;
 
   // SIMT paths
   void *d_simt_pc = nullptr;      // N x 21 x L probabilities (float or double)

@@ -44,6 +44,27 @@ __host__ __device__ constexpr int slot_of(int q, int l) {
   return (l / kGroupCols) * kGroupSlots + q * kGroupCols + (l % kGroupCols);
 }
 
+// The same permutation with a general group width, as a traits type: COLS
+// alignment columns per group of SLOTS slots, s(q, l) = (l / COLS) * SLOTS +
+// q * COLS + l % COLS, ones slot q = 21 of group 0 (slot 21 * COLS).
+//   Groups256: 12 columns per 256 slots (the layout above).
+//   Groups192: 9 columns per 192 slots, for the sparse integer forward, whose
+//              two 192-column s32 accumulators leave TMEM columns free for the
+//              sparsity metadata (two 256-column ones fill all 512).
+template <int COLS, int SLOTS>
+struct SlotGroups {
+  static constexpr int kCols = COLS;
+  static constexpr int kSlots = SLOTS;
+  static constexpr int kUsed = kQ * COLS;
+  static constexpr int kOnes = kQ * COLS;
+  __host__ __device__ static constexpr int groups(int L) { return (L + COLS - 1) / COLS; }
+  __host__ __device__ static constexpr int slot_of(int q, int l) {
+    return (l / COLS) * SLOTS + q * COLS + (l % COLS);
+  }
+};
+using Groups256 = SlotGroups<kGroupCols, kGroupSlots>;
+using Groups192 = SlotGroups<9, 192>;
+
 __host__ __device__ constexpr long long x2_index(int b, int k, int a, int j, int L) {
   return (((long long)b * L + k) * kQPad + a) * L + j;
 }

@@ -317,6 +317,58 @@ __device__ __forceinline__ void umma_i8_pair(uint32_t d_tmem, uint64_t a_desc, u
       : "memory");
 }
 
+// ------------------------------------------------ sparse integer MMA (2:4 on A)
+// Instruction descriptor bit 2: A is 2:4 structured-sparse, its metadata in TMEM.
+constexpr uint32_t kIdescSparse = 1u << 2;
+
+// Shared-memory descriptor, 32-byte swizzle (layout type 6).  MN-major: 32
+// MN-contiguous bytes per row, one row per K index; 8-row K groups SBO apart,
+// 32-byte MN atoms LBO apart.
+__device__ __forceinline__ uint64_t sdesc_sw32(uint32_t saddr, uint32_t lbo_bytes,
+                                               uint32_t sbo_bytes) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>((lbo_bytes >> 4) & 0x3FFFu) << 16;
+  d |= static_cast<uint64_t>((sbo_bytes >> 4) & 0x3FFFu) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  d |= static_cast<uint64_t>(6) << 61;
+  return d;
+}
+
+// Shared-memory descriptor without swizzle (layout type 0): core matrices of
+// 8 rows x 16 bytes stored as 128 contiguous bytes; 8-row groups SBO apart, core
+// matrices along K LBO apart.
+__device__ __forceinline__ uint64_t sdesc_noswz(uint32_t saddr, uint32_t lbo_bytes,
+                                                uint32_t sbo_bytes) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>((lbo_bytes >> 4) & 0x3FFFu) << 16;
+  d |= static_cast<uint64_t>((sbo_bytes >> 4) & 0x3FFFu) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  return d;
+}
+
+// Leader only: copy 128 rows x 16 bytes from shared memory (descriptor `src`, in
+// each CTA of the pair) to TMEM lanes 0..127, columns [taddr, taddr + 4), of the
+// same CTA.  Ordered with the MMAs issued after it by the same thread.
+__device__ __forceinline__ void tmem_cp_pair_128x128b(uint32_t taddr, uint64_t src) {
+  asm volatile("tcgen05.cp.cta_group::2.128x128b [%0], %1;" ::"r"(taddr), "l"(src) : "memory");
+}
+
+// Pair MMA (leader only) with 2:4-sparse A: D (+)= A * B, 8-bit integers,
+// K = 64 logical (32 stored bytes of A per row), metadata at TMEM column `meta`
+// (two columns per instruction: 4 bits per group of four logical K).
+__device__ __forceinline__ void umma_i8sp_pair(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
+                                               uint32_t idesc, uint32_t meta,
+                                               uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %5, 0;\n\t"
+      "tcgen05.mma.sp.cta_group::2.kind::i8 [%0], %1, %2, [%4], %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(meta), "r"(accumulate)
+      : "memory");
+}
+
 // 32 lanes x 32 columns of 32-bit, registers -> TMEM (the inverse of tmem_ld32).
 __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&r)[32]) {
   asm volatile(

@@ -93,27 +93,63 @@ __global__ void __launch_bounds__(256) i8_colmax_kernel(const float *__restrict_
   if (c < kQ * L && m > 0.0f) atomicMax(colmax + c, __float_as_uint(m));
 }
 
-// Per slot s: the encoding factor 2^(21 - e) of the digits of its coupling column
-// (e the column's exponent, from the maxima above), 0 for padding slots; read by prep.
+// Per slot s (of the slot groups G): the encoding factor 2^(21 - e) of the digits
+// of its coupling column (e the column's exponent, from the maxima above), 0 for
+// padding slots; read by prep.
+template <class G>
 __global__ void i8_scales_kernel(const uint32_t *__restrict__ colmax, float *__restrict__ enc,
                                  int L, int S) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= S) return;
-  const int t = s / kGroupSlots, r = s % kGroupSlots;
+  const int t = s / G::kSlots, r = s % G::kSlots;
   float f = 0.0f;
-  if (r < kGroupUsed) {
-    const int a = r / kGroupCols, j = t * kGroupCols + r % kGroupCols;
+  if (r < G::kUsed) {
+    const int a = r / G::kCols, j = t * G::kCols + r % G::kCols;
     if (j < L) f = pow2f(kI8FracBits - col_exponent(colmax[a * L + j]));
   }
   enc[s] = f;
 }
 
+// Operand storage of the sparse forward.  Every operand tile a stage needs is
+// stored contiguously in global memory as the exact shared-memory image the
+// MMA reads (swizzle included), so that one TMA box of 256-byte rows moves it;
+// tiles with 16-, 32- or 64-byte rows cost one TMA request per row and leave the
+// kernel bound by the L1/TMA request rate.  KB = KP / 128 K blocks.
+//   A (compressed one-hot, 128 rows x 64 bytes, 64-byte swizzle): tile
+//     (m128, kb) at ((m128 * KB + kb) * 128 + r) * 64; 16-byte chunk c of row r
+//     stored at chunk c ^ ((r >> 1) & 3).
+//   E (metadata, 128 rows x 16 bytes, no swizzle): tile (m128, kb) at
+//     ((m128 * KB + kb) * 128 + r) * 16.
+//   B (digits of W; per forward tile t and CTA half h, 128 K rows x 96 slots as
+//     three atoms of 32 slots, 32-byte swizzle): atom i at
+//     (((t * 2 + h) * KB + kb) * 3 + i) * 4096 + r * 32; chunk c of row r stored
+//     at chunk c ^ ((r >> 2) & 1).
+__host__ __device__ constexpr long long i8sp_a_offset(int n, int col, int KB) {
+  // col: byte of the compressed row (0 .. KP/2)
+  return (((long long)(n >> 7) * KB + (col >> 6)) * 128 + (n & 127)) * 64 +
+         ((((col >> 4) & 3) ^ (((n & 127) >> 1) & 3)) << 4) + (col & 15);
+}
+__host__ __device__ constexpr long long i8sp_e_offset(int n, int byte, int KB) {
+  return (((long long)(n >> 7) * KB + (byte >> 4)) * 128 + (n & 127)) * 16 + (byte & 15);
+}
+__host__ __device__ constexpr long long i8sp_b_offset(int kr, int s, int KB) {
+  // kr: K row (l * 21 + q), s: slot of the 192-slot groups
+  const int t = s / Groups192::kSlots, c = s % Groups192::kSlots;
+  const int h = c / 96, i = (c % 96) >> 5, x = c & 31, r = kr & 127;
+  return ((((long long)t * 2 + h) * KB + (kr >> 7)) * 3 + i) * 4096 + r * 32 +
+         ((((x >> 4) ^ (r >> 2)) & 1) << 4) + (x & 15);
+}
+
 // ---------------------------------------------------------------- prep
 // One block per row (b, k) of W, as tc_prep: g2 <- g2_coef * lambda2 * x, the FP64
-// partial of sum x^2, and row s(b, k) of the three digit matrices of Wperm (16
-// slots per thread, one 16-byte store per digit matrix).  The row is staged in
-// shared memory in slot order, so that the digit pass reads 16 consecutive slots
-// per thread (vector loads, no index arithmetic) with their per-slot factors.
+// partial of sum x^2, and one row of the three digit matrices of W (16 slots per
+// thread, one 16-byte store per digit matrix).  Columns are the slots of the
+// groups G; the row is s(b, k) (NAT = false: Wperm, both sides permuted) or
+// K row k * 21 + b of the sparse forward (NAT = true, alignment column major,
+// stored in its tiled layout).  args.S is the row length.  The row is staged in shared memory in slot order,
+// so that the digit pass reads 16 consecutive slots per thread (vector loads, no
+// index arithmetic) with their per-slot factors.
+template <class G, bool NAT>
 __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ x2,
                                                       float *__restrict__ g2, I8PrepArgs args) {
   extern __shared__ __align__(16) float xrow[];  // S floats: the row in slot order
@@ -151,7 +187,7 @@ __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ 
             const int j = c - a * L;
             const float vv[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
 #pragma unroll
-            for (int e = 0; e < 4; ++e) xrow[slot_of(a, j + e)] = vv[e];
+            for (int e = 0; e < 4; ++e) xrow[G::slot_of(a, j + e)] = vv[e];
           }
           __stcs(dst + i, make_float4(two_l2 * v[u].x, two_l2 * v[u].y, two_l2 * v[u].z,
                                       two_l2 * v[u].w));
@@ -162,12 +198,12 @@ __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ 
     for (int i = threadIdx.x; i < kQPad * L; i += blockDim.x) {
       const float v = x2[base + i];
       acc += (double)v * v;
-      if (i < nreal) xrow[slot_of(i / L, i % L)] = v;
+      if (i < nreal) xrow[G::slot_of(i / L, i % L)] = v;
       g2[base + i] = two_l2 * v;
     }
   }
   __syncthreads();
-  const long long srow = (long long)slot_of(b, k) * args.S;
+  const long long srow = (long long)G::slot_of(b, k) * args.S;  // (NAT: tiled, i8sp_b_offset)
   for (int u = threadIdx.x; u < args.S / 16; u += blockDim.x) {
     uint32_t p0[4], p1[4], p2[4];
 #pragma unroll
@@ -190,7 +226,7 @@ __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ 
       p1[e4] = pack(qv[0] >> 7, qv[1] >> 7, qv[2] >> 7, qv[3] >> 7) & 0x7F7F7F7Fu;
       p2[e4] = pack(qv[0], qv[1], qv[2], qv[3]) & 0x7F7F7F7Fu;
     }
-    const long long off = srow + (long long)u * 16;
+    const long long off = NAT ? i8sp_b_offset(k * kQ + b, u * 16, args.KB) : srow + (long long)u * 16;
     *reinterpret_cast<uint4 *>(args.wdig[0] + off) = make_uint4(p0[0], p0[1], p0[2], p0[3]);
     *reinterpret_cast<uint4 *>(args.wdig[1] + off) = make_uint4(p1[0], p1[1], p1[2], p1[3]);
     *reinterpret_cast<uint4 *>(args.wdig[2] + off) = make_uint4(p2[0], p2[1], p2[2], p2[3]);
@@ -206,21 +242,22 @@ __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ 
   }
 }
 
-// One-hot operands of the integer path: O1[n][s] = 1 and O128[n][s] = 128 where
-// the state of column l(s) in row n is q(s), and in the ones slot of every real
-// row; 0 elsewhere.
+// One-hot operands of the integer path (slot groups G): O1[n][s] = 1 and
+// O128[n][s] = 128 where the state of column l(s) in row n is q(s), and in the
+// ones slot of every real row; 0 elsewhere.
+template <class G>
 __global__ void i8_onehot_kernel(const uint8_t *__restrict__ msa, uint8_t *__restrict__ o1,
                                  uint8_t *__restrict__ o128, int L, int N, int S, int Npad) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long long)Npad * S) return;
   const int n = (int)(idx / S), s = (int)(idx % S);
-  const int t = s / kGroupSlots, r = s % kGroupSlots;
+  const int t = s / G::kSlots, r = s % G::kSlots;
   bool one = false;
   if (n < N) {
-    if (s == kOnesSlot) {
+    if (s == G::kOnes) {
       one = true;
-    } else if (r < kGroupUsed) {
-      const int q = r / kGroupCols, l = t * kGroupCols + r % kGroupCols;
+    } else if (r < G::kUsed) {
+      const int q = r / G::kCols, l = t * G::kCols + r % G::kCols;
       one = l < L && msa[(long long)n * L + l] == q;
     }
   }
@@ -268,12 +305,16 @@ struct I8FwdSmem {
 //          M = max(m, m'), S = s exp(m - M) + s' exp(m' - M) (same order in both
 //          halves), lse = M + log S;
 //   C:     P = e * exp(m - M) / S, R = w (P - onehot) as its three digits.
-template <int H>
+// G: the slot groups of the tile (one group = one tile, G::kSlots columns, half
+// of them per warp).
+template <class G, int H>
 __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint32_t t_hi,
                                                      uint32_t t_lo, const float *tab_scale,
                                                      const float *tab_v, float *xbuf, int q,
                                                      int lane, int n, int t, long long part,
                                                      uint32_t lo_bar) {
+  constexpr int kGroupCols = G::kCols, kGroupUsed = G::kUsed;
+  constexpr int kChunks = G::kSlots / 64;  // 32-column chunks per half
   const int L = args.L;
   const int j0 = t * kGroupCols;
   const bool live = n < args.N;
@@ -291,8 +332,8 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
   for (int jj = 0; jj < kGroupCols; ++jj) { mx[jj] = -INFINITY; tg[jj] = 0.0f; se[jj] = 0.0f; }
   // merge + maxima
 #pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const int cc = 4 * H + c;
+  for (int c = 0; c < kChunks; ++c) {
+    const int cc = kChunks * H + c;
     uint32_t vh[32], vl[32];
     __syncwarp();
     tmem_ld32(t_hi + cc * 32, vh);
@@ -318,8 +359,8 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
   if (lane == 0) mbar_arrive_cluster(lo_bar);  // the next tile's low phase may start
   // B: e = exp(z - m), sum
 #pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const int cc = 4 * H + c;
+  for (int c = 0; c < kChunks; ++c) {
+    const int cc = kChunks * H + c;
     uint32_t v[32];
     __syncwarp();
     tmem_ld32(t_hi + cc * 32, v);
@@ -356,15 +397,15 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
     const float S = H == 0 ? se[jj] * fa + so * fo : so * fo + se[jj] * fa;
     const float lse = M + logf(S);
     cw[jj] = xr[jj] >= 0 ? (fa / S) * won : 0.0f;
-    if (xr[jj] >= 0 && ((xr[jj] * kGroupCols + jj) >> 7) == H)
+    if (xr[jj] >= 0 && (xr[jj] * kGroupCols + jj) / (G::kSlots / 2) == H)
       floss += (double)(wn * (lse - tg[jj]));
   }
   tmem_wait_st();
   // C: R = w (P - onehot), three digits per element
-  const long long rbase = (long long)n * args.S + (long long)t * kGroupSlots;
+  const long long rbase = (long long)n * args.S + (long long)t * G::kSlots;
 #pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const int cc = 4 * H + c;
+  for (int c = 0; c < kChunks; ++c) {
+    const int cc = kChunks * H + c;
     uint32_t v[32];
     __syncwarp();
     tmem_ld32(t_hi + cc * 32, v);
@@ -590,11 +631,304 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
       const uint32_t lq = (uint32_t)(q * 32) << 16;
       const long long part = (long long)tile * 2 + rank;
       if (half == 0)
-        i8_fwd_epilogue_tile<0>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v, xbuf, q, lane, n, t,
+        i8_fwd_epilogue_tile<Groups256, 0>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v, xbuf, q, lane, n, t,
                                 part, lo_bar);
       else
-        i8_fwd_epilogue_tile<1>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v, xbuf, q, lane, n, t,
+        i8_fwd_epilogue_tile<Groups256, 1>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v, xbuf, q, lane, n, t,
                                 part, lo_bar);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(hi_bar);
+    }
+  }
+
+  tc_fence_before();
+  cluster_sync();
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc_pair(tmem_base, 512);
+  }
+}
+
+// ---------------------------------------------------------------- sparse forward
+// CCM_PATH_TC_I8SP.  The one-hot operand with its K order changed to
+// k' = l * 21 + q (alignment column major): any four consecutive k' span at most
+// two alignment columns, and a row has exactly one 1 per column, so every group
+// of four holds at most two ones -- the 2:4 structured sparsity that
+// tcgen05.mma.sp runs at twice the dense rate.  A is stored compressed (the two
+// kept values of each group) with 4 bits of metadata per group: the kept
+// positions i0 < i1 in bits 0-1 and 2-3, group c of a row in nibble c of the
+// row's metadata bytes (low nibble first).  A group with a single 1 keeps it
+// with a zero partner, an empty group keeps (0, 1) with two zeros.
+// One thread per metadata byte (two groups, eight logical K).
+__global__ void i8sp_onehot_kernel(const uint8_t *__restrict__ msa, uint32_t *__restrict__ ac1,
+                                   uint32_t *__restrict__ ac128, uint8_t *__restrict__ meta,
+                                   int L, int N, int KP, int Npad) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nb = KP / 8;
+  if (idx >= (long long)Npad * nb) return;
+  const int n = (int)(idx / nb), byte = (int)(idx % nb);
+  uint32_t vals = 0, m = 0;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int c = 2 * byte + h;
+    int pos[2] = {0, 0}, cnt = 0;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      const int k = 4 * c + p;
+      if (n < N && k < kQ * L && msa[(long long)n * L + k / kQ] == k % kQ) {
+        if (cnt < 2) pos[cnt] = p;
+        ++cnt;
+      }
+    }
+    int i0 = 0, i1 = 1, v0 = 0, v1 = 0;
+    if (cnt >= 2) {
+      i0 = pos[0]; i1 = pos[1]; v0 = 1; v1 = 1;
+    } else if (cnt == 1) {
+      if (pos[0] < 3) { i0 = pos[0]; i1 = 3; v0 = 1; }
+      else { i0 = 2; i1 = 3; v1 = 1; }
+    }
+    m |= (uint32_t)(i0 | (i1 << 2)) << (4 * h);
+    vals |= (uint32_t)(v0 | (v1 << 8)) << (16 * h);
+  }
+  // compressed row n: KP / 2 bytes, four per metadata byte (one aligned word)
+  const int KB = KP / 128;
+  meta[i8sp_e_offset(n, byte, KB)] = (uint8_t)m;
+  const long long ao = i8sp_a_offset(n, 4 * byte, KB) >> 2;
+  ac1[ao] = vals;
+  ac128[ao] = vals * 128;  // the same with values 128
+}
+
+// As i8_forward_kernel on 256 x 192 tiles (Groups192, nine alignment columns per
+// tile), with sparse MMAs (K = 64 logical per instruction).  Per 128 logical K
+// the CTA holds A compressed as 128 rows x 64 bytes (64-byte swizzle), the
+// metadata as 128 rows x 16 bytes (no swizzle), copied into TMEM by tcgen05.cp
+// ahead of the MMAs that read it (the copy and the MMAs issue from one thread and
+// execute in order; two metadata slots alternate), and B -- the digits of W with
+// rows in the K order k' -- MN-major, 96 columns per CTA as three 32-byte
+// swizzled atoms of 128 K rows.  Each of these is one TMA box of the tiled
+// storage above (no TMA swizzle: the images are stored swizzled).  TMEM: hi = [0, 192), lo = [256, 448), metadata
+// slots at 448 and 452.
+constexpr int kSpBN = Groups192::kSlots, kSpBK = 128;
+
+struct I8SpSmem {
+  static constexpr int kStages = 4;
+  static constexpr int kA = kI8BM * kSpBK / 2;  // 8 KB
+  static constexpr int kAtom = kSpBK * 32;      // 4 KB: 128 K rows x 32 columns
+  static constexpr int kB = 3 * kAtom;          // 12 KB: 96 columns
+  static constexpr int kE = kI8BM * kSpBK / 8;  // 2 KB
+  // low phase (one K block):   A x128 | A x1 | B d1 | B d2 | E
+  // high phase (two K blocks): A x1 (kb) | A x1 (kb+1) | B d0 (kb) | B d0 (kb+1) | E (kb) | E (kb+1)
+  static constexpr int kOffA0 = 0, kOffA1 = kA, kOffB0 = 2 * kA, kOffB1 = 2 * kA + kB;
+  static constexpr int kOffE0 = 2 * kA + 2 * kB, kOffE1 = kOffE0 + kE;
+  static constexpr int kStage = kOffE1 + kE;
+  static constexpr int kBarOff = kStages * kStage;
+  static constexpr int kTabOff = kBarOff + 256;  // per tile: scale[192], V[192]
+  static constexpr int kXOff = kTabOff + 2 * kSpBN * 4;
+  static constexpr int kXBytes = 2 * kI8BM * 2 * Groups192::kCols * 4;
+  static constexpr int kTotal = kXOff + kXBytes + 1024;
+};
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
+    i8sp_forward_kernel(const __grid_constant__ I8SpMaps maps, I8FwdArgs args) {
+  using SM = I8SpSmem;
+  constexpr int kStages = SM::kStages;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = i8_align1024(smem_raw);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + SM::kBarOff);
+  uint64_t *empty = full + kStages;
+  uint64_t *acc_full = empty + kStages;
+  uint64_t *lo_empty = acc_full + 1;
+  uint64_t *hi_empty = lo_empty + 1;
+  uint64_t *drain = hi_empty + 1;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+  float *tab_scale = reinterpret_cast<float *>(smem + SM::kTabOff);
+  float *tab_v = tab_scale + kSpBN;
+  float *xbuf = reinterpret_cast<float *>(smem + SM::kXOff);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
+  const int n_tiles = args.m_tiles * args.T;
+  const int k_blocks = args.KP / kSpBK;  // even
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+    mbar_init(acc_full, 1);
+    mbar_init(lo_empty, 16);
+    mbar_init(hi_empty, 16);
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&maps.a1);
+    prefetch_tmap(&maps.a128);
+    prefetch_tmap(&maps.e);
+    for (int i = 0; i < 3; ++i) prefetch_tmap(&maps.b[i]);
+  }
+  if (warp == 1) { tmem_alloc_pair(tmem_slot, 512); tmem_relinquish_pair(); }
+  tc_fence_before();
+  cluster_sync();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  const uint32_t t_hi = tmem_base, t_lo = tmem_base + 256, t_e = tmem_base + 448;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---------------- TMA producer (both CTAs), in the MMA's order
+      uint32_t it = 0;
+      bool ok = true;
+      for (int tile = pair; tile < n_tiles && ok && !i8_aborted(abort_flag); tile += npairs) {
+        const int m = tile % args.m_tiles, t = tile / args.m_tiles;
+        // tile rows of the tiled operands (256-byte rows): A 32, E 8, B 48 per K block
+        const int m128 = 2 * m + (int)rank, tb = 2 * t + (int)rank;
+        for (int phase = 0; phase < 2 && ok; ++phase) {  // 0: low digits, 1: high digit
+          for (int kb = 0; kb < k_blocks; kb += (phase == 0 ? 1 : 2), ++it) {
+            const int stage = it % kStages;
+            const uint32_t round = it / kStages;
+            if (!mbar_wait(&empty[stage], (round & 1) ^ 1)) {
+              i8_record_error(args.status, kErrFwdTimeout, abort_flag);
+              ok = false;
+              break;
+            }
+            uint8_t *st = smem + stage * SM::kStage;
+            const uint32_t fb = mapa_shared(smem_u32(&full[stage]), 0);
+            if (phase == 0) {
+              if (rank == 0) mbar_arrive_expect_tx(&full[stage], 2 * (2 * SM::kA + 2 * SM::kB + SM::kE));
+              tma_load_2d_pair(st + SM::kOffA0, &maps.a128, fb, 0, (m128 * k_blocks + kb) * 32);
+              tma_load_2d_pair(st + SM::kOffA1, &maps.a1, fb, 0, (m128 * k_blocks + kb) * 32);
+              tma_load_2d_pair(st + SM::kOffB0, &maps.b[1], fb, 0, (tb * k_blocks + kb) * 48);
+              tma_load_2d_pair(st + SM::kOffB1, &maps.b[2], fb, 0, (tb * k_blocks + kb) * 48);
+              tma_load_2d_pair(st + SM::kOffE0, &maps.e, fb, 0, (m128 * k_blocks + kb) * 8);
+            } else {
+              if (rank == 0) mbar_arrive_expect_tx(&full[stage], 2 * SM::kStage);
+              for (int sub = 0; sub < 2; ++sub) {
+                const int k2 = kb + sub;
+                tma_load_2d_pair(st + sub * SM::kA, &maps.a1, fb, 0, (m128 * k_blocks + k2) * 32);
+                tma_load_2d_pair(st + SM::kOffB0 + sub * SM::kB, &maps.b[0], fb, 0,
+                                 (tb * k_blocks + k2) * 48);
+                tma_load_2d_pair(st + SM::kOffE0 + sub * SM::kE, &maps.e, fb, 0,
+                                 (m128 * k_blocks + k2) * 8);
+              }
+            }
+          }
+        }
+      }
+      const uint32_t issued = it;
+      for (uint32_t r = (issued > kStages ? issued - kStages : 0); r < issued; ++r) {
+        const bool w = rank == 0 ? mbar_wait(&full[r % kStages], (r / kStages) & 1)
+                                 : mbar_wait(&empty[r % kStages], (r / kStages) & 1);
+        if (!w) {
+          i8_record_error(args.status, kErrFwdTimeout, abort_flag);
+          break;
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && rank == 0) {
+      // ---------------- MMA issuer (leader): 256 x 192 x 64 (logical) sparse pair MMAs
+      constexpr uint32_t idesc = idesc_i8_s32(kI8PairM, kSpBN, 0, 1, 0, 1) | kIdescSparse;
+      uint32_t it = 0, ecopies = 0;
+      int local = 0;
+      bool ok = true;
+      for (int tile = pair; tile < n_tiles && ok && !i8_aborted(abort_flag);
+           tile += npairs, ++local) {
+        const uint32_t wpar = (local & 1) ^ 1;
+        for (int phase = 0; phase < 2 && ok; ++phase) {
+          if (!mbar_wait(phase == 0 ? lo_empty : hi_empty, wpar)) {
+            i8_record_error(args.status, kErrFwdTimeout, abort_flag);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          for (int kb = 0; kb < k_blocks; kb += (phase == 0 ? 1 : 2), ++it) {
+            const int stage = it % kStages;
+            const uint32_t round = it / kStages;
+            if (!mbar_wait(&full[stage], round & 1)) {
+              i8_record_error(args.status, kErrFwdTimeout, abort_flag);
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t s0 = smem_u32(smem + stage * SM::kStage);
+            if (phase == 0) {
+              const uint32_t te = t_e + 4 * (ecopies++ & 1);
+              tmem_cp_pair_128x128b(te, sdesc_noswz(s0 + SM::kOffE0, 2048, 128));
+#pragma unroll
+              for (int k = 0; k < 2; ++k) {
+                const uint64_t a128 = sdesc_sw64(s0 + SM::kOffA0 + k * 32, 16, 512);
+                const uint64_t a1 = sdesc_sw64(s0 + SM::kOffA1 + k * 32, 16, 512);
+                const uint64_t bA = sdesc_sw32(s0 + SM::kOffB0 + k * 2048, SM::kAtom, 256);
+                const uint64_t bB = sdesc_sw32(s0 + SM::kOffB1 + k * 2048, SM::kAtom, 256);
+                umma_i8sp_pair(t_lo, a128, bA, idesc, te + 2 * k, (kb | k) != 0);
+                umma_i8sp_pair(t_lo, a1, bB, idesc, te + 2 * k, 1);
+              }
+            } else {
+#pragma unroll
+              for (int sub = 0; sub < 2; ++sub) {
+                const uint32_t te = t_e + 4 * (ecopies++ & 1);
+                tmem_cp_pair_128x128b(te, sdesc_noswz(s0 + SM::kOffE0 + sub * SM::kE, 2048, 128));
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                  const uint64_t a1 = sdesc_sw64(s0 + sub * SM::kA + k * 32, 16, 512);
+                  const uint64_t b0 =
+                      sdesc_sw32(s0 + SM::kOffB0 + sub * SM::kB + k * 2048, SM::kAtom, 256);
+                  umma_i8sp_pair(t_hi, a1, b0, idesc, te + 2 * k, (kb | sub | k) != 0);
+                }
+              }
+            }
+            umma_commit_pair(&empty[stage], 0x3);
+          }
+        }
+        if (ok) umma_commit_pair(acc_full, 0x3);
+      }
+      umma_commit_pair(drain, 0x1);
+      if (!mbar_wait(drain, 0)) i8_record_error(args.status, kErrFwdTimeout, abort_flag);
+    }
+  } else {
+    // ---------------- epilogue (both CTAs): 8 warps, lane quarter q, column half
+    const int q = warp & 3;
+    const int half = (warp - 2) >> 2;
+    const int ethr = threadIdx.x - 64;
+    const int L = args.L;
+    const uint32_t lo_bar = mapa_shared(smem_u32(lo_empty), 0);
+    const uint32_t hi_bar = mapa_shared(smem_u32(hi_empty), 0);
+    int local = 0;
+    for (int tile = pair; tile < n_tiles; tile += npairs, ++local) {
+      if (named_bar_or(1, 256, i8_aborted(abort_flag))) break;
+      const int m = tile % args.m_tiles, t = tile / args.m_tiles;
+      if (ethr < kSpBN) {
+        const int r = ethr;
+        float sc = 0.0f, vv = 0.0f;
+        if (r < Groups192::kUsed) {
+          const int a = r / Groups192::kCols, j = t * Groups192::kCols + r % Groups192::kCols;
+          if (j < L) {
+            sc = pow2f(col_exponent(args.colmax[a * L + j]) - kI8FracBits);
+            if (a < kQ - 1) vv = args.x1[a * L + j];
+          }
+        }
+        tab_scale[r] = sc;
+        tab_v[r] = vv;
+      }
+      named_bar_sync(1, 256);
+      const int n = m * kI8PairM + (int)rank * kI8BM + q * 32 + lane;
+      const bool ok = mbar_wait(acc_full, local & 1);
+      if (__any_sync(0xffffffffu, !ok)) {
+        if (lane == 0) i8_record_error(args.status, kErrFwdTimeout, abort_flag);
+        continue;
+      }
+      tc_fence_after();
+      const uint32_t lq = (uint32_t)(q * 32) << 16;
+      const long long part = (long long)tile * 2 + rank;
+      if (half == 0)
+        i8_fwd_epilogue_tile<Groups192, 0>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v, xbuf, q,
+                                           lane, n, t, part, lo_bar);
+      else
+        i8_fwd_epilogue_tile<Groups192, 1>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v, xbuf, q,
+                                           lane, n, t, part, lo_bar);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive_cluster(hi_bar);
@@ -638,7 +972,7 @@ struct I8BwdSmem {
   static constexpr int kTotal = kTOff + kTBytes + 1024;
 };
 
-template <bool SYM>
+template <bool SYM, class G>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
     i8_backward_kernel(const __grid_constant__ I8BwdMaps maps, BwdArgs args) {
   using SM = I8BwdSmem;
@@ -814,13 +1148,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
       const int2 pq = args.tiles[tile];
       const int rowbase = pq.x * kPairM + (int)rank * kBM + q * 32;
       const int s1 = rowbase + lane;
-      const int t1 = s1 / kGroupSlots, r1 = s1 % kGroupSlots;
-      const int b = r1 / kGroupCols, k = t1 * kGroupCols + r1 % kGroupCols;
-      const bool valid1 = r1 < kGroupUsed && k < L;
+      const int t1 = s1 / G::kSlots, r1 = s1 % G::kSlots;
+      const int b = r1 / G::kCols, k = t1 * G::kCols + r1 % G::kCols;
+      const bool valid1 = r1 < G::kUsed && k < L;
       const long long colt = (long long)b * L + k;
-      const int tQ = pq.y * kBN / kGroupSlots;
-      const int rQ = pq.y * kBN % kGroupSlots + half * kHalfN;
-      const int sQ = tQ * kGroupSlots + rQ;
+      // the Q slots of this warp: sQ + i, i < 128 (with 192-slot groups a 256-slot
+      // tile half may cross a group boundary: decode each slot on its own)
+      const int sQ = pq.y * kBN + half * kHalfN;
 #pragma unroll
       for (int cb = 0; cb < kHalfN / 8; ++cb) {
         __syncwarp();
@@ -830,36 +1164,36 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
         if (SYM) {
 #pragma unroll 1
           for (int col = 0; col < 8; ++col) {
-            const int r2 = rQ + cb * 8 + col;
             const int s2 = sQ + cb * 8 + col;
-            const int a = r2 / kGroupCols, j = tQ * kGroupCols + r2 % kGroupCols;
-            const bool valid2 = r2 < kGroupUsed && j < L;
+            const int t2 = s2 / G::kSlots, r2 = s2 % G::kSlots;
+            const int a = r2 / G::kCols, j = t2 * G::kCols + r2 % G::kCols;
+            const bool valid2 = r2 < G::kUsed && j < L;
             if (s1 < s2) {
               const float val = Tb[lane * 9 + col];
               if (valid1 && valid2) {
                 if (k != j) atomicAdd(g2 + ((long long)a * L + j) * kQPad * L + colt, val);
-              } else if (s2 == kOnesSlot && valid1 && b < kQ - 1) {
+              } else if (s2 == G::kOnes && valid1 && b < kQ - 1) {
                 args.g1d[b * L + k] = val;
               }
             }
           }
         }
         const int col = lane & 7;
-        const int r2 = rQ + cb * 8 + col;
         const int s2 = sQ + cb * 8 + col;
-        const int a = r2 / kGroupCols, j = tQ * kGroupCols + r2 % kGroupCols;
-        const bool valid2 = r2 < kGroupUsed && j < L;
+        const int t2 = s2 / G::kSlots, r2 = s2 % G::kSlots;
+        const int a = r2 / G::kCols, j = t2 * G::kCols + r2 % G::kCols;
+        const bool valid2 = r2 < G::kUsed && j < L;
 #pragma unroll
         for (int it = 0; it < 8; ++it) {
           const int row = 4 * it + (lane >> 3);
           const int s1r = rowbase + row;
           if (SYM && s1r > s2) continue;
           const float val = Tb[row * 9 + col];
-          const int tr = s1r / kGroupSlots, rr = s1r % kGroupSlots;
-          const int br = rr / kGroupCols, kr = tr * kGroupCols + rr % kGroupCols;
-          if (rr < kGroupUsed && kr < L) {
+          const int tr = s1r / G::kSlots, rr = s1r % G::kSlots;
+          const int br = rr / G::kCols, kr = tr * G::kCols + rr % G::kCols;
+          if (rr < G::kUsed && kr < L) {
             if (valid2 && (!SYM || kr != j)) atomicAdd(g2 + x2_index(br, kr, a, j, L), val);
-          } else if (s1r == kOnesSlot && valid2 && a < kQ - 1) {
+          } else if (s1r == G::kOnes && valid2 && a < kQ - 1) {
             args.g1d[a * L + j] = val;
           }
         }
@@ -888,6 +1222,7 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
                         const double *d_alpha, float *d_xt) {
   const int L = c->L;
   const bool step = d_s != nullptr;
+  const bool sp = c->path == CCM_PATH_TC_I8SP;
   const float *xe = step ? d_xt : d_x;
   const float *x1 = xe;
   const float *x2 = xe + c->nsp;
@@ -907,16 +1242,26 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
                                                            c->d_colmax, L, c->nsp, kRows);
   // per-slot factors after the column maxima, 16-byte aligned for the float4 loads
   float *enc = reinterpret_cast<float *>(c->d_colmax + ((kQ * L + 3) & ~3));
-  i8_scales_kernel<<<(c->S + 255) / 256, 256, 0, c->stream>>>(c->d_colmax, enc, L, c->S);
+  // W digit rows: S slots (dense forward) or SW slots of 192-slot groups (sparse)
+  const int wcols = sp ? c->SW : c->S;
+  if (sp)
+    i8_scales_kernel<Groups192><<<(wcols + 255) / 256, 256, 0, c->stream>>>(c->d_colmax, enc, L,
+                                                                             wcols);
+  else
+    i8_scales_kernel<Groups256><<<(wcols + 255) / 256, 256, 0, c->stream>>>(c->d_colmax, enc, L,
+                                                                             wcols);
   I8PrepArgs pa{};
   for (int i = 0; i < 3; ++i) pa.wdig[i] = c->d_wdig[i];
   pa.colmax = c->d_colmax;
   pa.enc = enc;
   pa.part_reg = c->d_part_reg;
-  pa.L = L; pa.S = c->S; pa.lambda_pair = c->lambda_pair;
+  pa.L = L; pa.S = wcols; pa.KB = c->KP / 128; pa.lambda_pair = c->lambda_pair;
   pa.g2_coef = c->gradient == CCM_GRADIENT_PARTIAL ? 1.0f : 2.0f;
   pa.inv_L = 1.0f / (float)L;
-  i8_prep_kernel<<<kQ * L, 256, sizeof(float) * c->S, c->stream>>>(x2, g2, pa);
+  if (sp)
+    i8_prep_kernel<Groups192, true><<<kQ * L, 256, sizeof(float) * wcols, c->stream>>>(x2, g2, pa);
+  else
+    i8_prep_kernel<Groups256, false><<<kQ * L, 256, sizeof(float) * wcols, c->stream>>>(x2, g2, pa);
   prof_mark(c);
 
   I8FwdArgs fa{};
@@ -925,9 +1270,13 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   fa.part_f = c->d_part_f; fa.status = c->d_status;
   fa.L = L; fa.N = c->N; fa.S = c->S; fa.T = c->T; fa.Npad = c->Npad;
   fa.m_tiles = c->Npad / kI8PairM;
+  fa.KP = c->KP;
   const int pair_tiles = fa.m_tiles * c->T;
   const int fpairs = pair_tiles < c->fwd_pairs ? pair_tiles : c->fwd_pairs;
-  i8_forward_kernel<<<2 * fpairs, kI8Threads, I8FwdSmem::kTotal, c->stream>>>(c->i8fwd_maps, fa);
+  if (sp)
+    i8sp_forward_kernel<<<2 * fpairs, kI8Threads, I8SpSmem::kTotal, c->stream>>>(c->i8sp_maps, fa);
+  else
+    i8_forward_kernel<<<2 * fpairs, kI8Threads, I8FwdSmem::kTotal, c->stream>>>(c->i8fwd_maps, fa);
   prof_mark(c);
 
   BwdArgs ba{};
@@ -935,12 +1284,20 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   ba.n_tiles = c->n_bwd_tiles; ba.status = c->d_status; ba.L = L; ba.S = c->S; ba.Npad = c->Npad;
   ba.lambda_pair = c->lambda_pair;
   const int bpairs = c->n_bwd_tiles < c->bwd_pairs ? c->n_bwd_tiles : c->bwd_pairs;
-  if (c->gradient == CCM_GRADIENT_PARTIAL)
-    i8_backward_kernel<false>
-        <<<2 * bpairs, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
+  const bool sym = c->gradient != CCM_GRADIENT_PARTIAL;
+  const dim3 bgrid(2 * bpairs);
+  if (sp && sym)
+    i8_backward_kernel<true, Groups192>
+        <<<bgrid, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
+  else if (sp)
+    i8_backward_kernel<false, Groups192>
+        <<<bgrid, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
+  else if (sym)
+    i8_backward_kernel<true, Groups256>
+        <<<bgrid, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
   else
-    i8_backward_kernel<true>
-        <<<2 * bpairs, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
+    i8_backward_kernel<false, Groups256>
+        <<<bgrid, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
   prof_mark(c);
 
   launch_tc_finalize(c, x1, d_g, 2LL * pair_tiles);
@@ -951,20 +1308,28 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
 
 cudaError_t i8_configure_kernels() {
   cudaError_t e;
+  const int kMax = cudaFuncAttributeMaxDynamicSharedMemorySize;
   // the staged row is S floats: up to L = 2688 (the 227 KB per block, less the
   // kernel's static reduction buffer)
-  if ((e = cudaFuncSetAttribute(i8_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if ((e = cudaFuncSetAttribute(i8_prep_kernel<Groups256, false>, (cudaFuncAttribute)kMax,
+                                230000)) != cudaSuccess ||
+      (e = cudaFuncSetAttribute(i8_prep_kernel<Groups192, true>, (cudaFuncAttribute)kMax,
                                 230000)) != cudaSuccess)
     return e;
-  if ((e = cudaFuncSetAttribute(i8_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                I8FwdSmem::kTotal)) != cudaSuccess)
+  if ((e = cudaFuncSetAttribute(i8_forward_kernel, (cudaFuncAttribute)kMax, I8FwdSmem::kTotal)) !=
+          cudaSuccess ||
+      (e = cudaFuncSetAttribute(i8sp_forward_kernel, (cudaFuncAttribute)kMax, I8SpSmem::kTotal)) !=
+          cudaSuccess)
     return e;
-  if ((e = cudaFuncSetAttribute(i8_backward_kernel<true>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if ((e = cudaFuncSetAttribute(i8_backward_kernel<true, Groups256>, (cudaFuncAttribute)kMax,
+                                I8BwdSmem::kTotal)) != cudaSuccess ||
+      (e = cudaFuncSetAttribute(i8_backward_kernel<false, Groups256>, (cudaFuncAttribute)kMax,
+                                I8BwdSmem::kTotal)) != cudaSuccess ||
+      (e = cudaFuncSetAttribute(i8_backward_kernel<true, Groups192>, (cudaFuncAttribute)kMax,
                                 I8BwdSmem::kTotal)) != cudaSuccess)
     return e;
-  return cudaFuncSetAttribute(i8_backward_kernel<false>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, I8BwdSmem::kTotal);
+  return cudaFuncSetAttribute(i8_backward_kernel<false, Groups192>, (cudaFuncAttribute)kMax,
+                              I8BwdSmem::kTotal);
 }
 
 cudaError_t i8_forward_max_pairs(int *pairs) {
@@ -976,20 +1341,40 @@ cudaError_t i8_forward_max_pairs(int *pairs) {
   return cudaOccupancyMaxActiveClusters(pairs, i8_forward_kernel, &cfg);
 }
 
+cudaError_t i8sp_forward_max_pairs(int *pairs) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2, 1, 1);
+  cfg.blockDim = dim3(kI8Threads, 1, 1);
+  cfg.dynamicSmemBytes = I8SpSmem::kTotal;
+  *pairs = 0;
+  return cudaOccupancyMaxActiveClusters(pairs, i8sp_forward_kernel, &cfg);
+}
+
 cudaError_t i8_backward_max_pairs(int *pairs) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(2, 1, 1);
   cfg.blockDim = dim3(kI8Threads, 1, 1);
   cfg.dynamicSmemBytes = I8BwdSmem::kTotal;
   *pairs = 0;
-  return cudaOccupancyMaxActiveClusters(pairs, i8_backward_kernel<true>, &cfg);
+  return cudaOccupancyMaxActiveClusters(pairs, i8_backward_kernel<true, Groups256>, &cfg);
 }
 
-// One-hot operands for a context of the integer path (Npad x S bytes each).
+// One-hot operands for a context of the integer paths (Npad x S bytes each), and
+// for the sparse path the compressed forward operand with its metadata.
 cudaError_t i8_build_onehot(ccm_context *c) {
   const long long total = (long long)c->Npad * c->S;
-  i8_onehot_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c->stream>>>(
-      c->d_msa, c->d_o1, c->d_o128, c->L, c->N, c->S, c->Npad);
+  const unsigned grid = (unsigned)((total + 255) / 256);
+  if (c->path != CCM_PATH_TC_I8SP) {
+    i8_onehot_kernel<Groups256><<<grid, 256, 0, c->stream>>>(c->d_msa, c->d_o1, c->d_o128, c->L,
+                                                             c->N, c->S, c->Npad);
+    return cudaGetLastError();
+  }
+  i8_onehot_kernel<Groups192><<<grid, 256, 0, c->stream>>>(c->d_msa, c->d_o1, c->d_o128, c->L,
+                                                           c->N, c->S, c->Npad);
+  const long long bytes = (long long)c->Npad * (c->KP / 8);
+  i8sp_onehot_kernel<<<(unsigned)((bytes + 255) / 256), 256, 0, c->stream>>>(
+      c->d_msa, reinterpret_cast<uint32_t *>(c->d_ac1), reinterpret_cast<uint32_t *>(c->d_ac128),
+      c->d_meta, c->L, c->N, c->KP, c->Npad);
   return cudaGetLastError();
 }
 

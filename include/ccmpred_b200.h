@@ -61,6 +61,8 @@ extern "C" {
 #define CCM_PATH_SIMT_F64 3  /* FP64 CUDA-core path (gradient checks) */
 #define CCM_PATH_TC_I8X3 4   /* tcgen05 kind::i8: W and R as three 8-bit fixed-point digits
                                 (21 fractional bits), exact s32 accumulation */
+#define CCM_PATH_TC_I8SP 5   /* CCM_PATH_TC_I8X3 with the forward on 2:4-sparse tcgen05.mma.sp
+                                (the one-hot operand compressed); the same exact sums */
 
 /* gradient conventions */
 #define CCM_GRADIENT_TIED 0    /* the reference's g: coupling part along the tied direction

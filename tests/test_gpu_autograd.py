@@ -67,7 +67,7 @@ def test_central_differences_500_coordinates_fp64(gpu):
     ev.close()
 
 
-@pytest.mark.parametrize("path", ["tc_i8x3", "tc_bf16x2", "simt_f32"])
+@pytest.mark.parametrize("path", ["tc_i8x3", "tc_i8sp", "tc_bf16x2", "simt_f32"])
 def test_partial_symmetrised_matches_reference_fp32(gpu, path):
     """FP32: partial + partial^T (k != j) equals the reference's evaluate_cpu
     gradient (golden vector, symmetric x)."""

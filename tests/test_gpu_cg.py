@@ -11,7 +11,7 @@ from ccmpred_b200.host import init_bias
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("path", ["tc_i8x3", "tc_bf16x2", "simt_f32"])
+@pytest.mark.parametrize("path", ["tc_i8x3", "tc_i8sp", "tc_bf16x2", "simt_f32"])
 def test_cg_matches_fp64_host_cg(gpu, oracle_mod, path):
     import torch
     msa = synth.generate(synth.MSAConfig("cg", 24, 300, n_pairs=4, dup_frac=0.2, seed=61))
@@ -75,7 +75,7 @@ def planted_pairs(cfg):
     return {(int(min(a, b)), int(max(a, b))) for a, b in cols}
 
 
-@pytest.mark.parametrize("path", ["tc_i8x3", "tc_bf16x2", "tc_bf16x3", "simt_f32"])
+@pytest.mark.parametrize("path", ["tc_i8x3", "tc_i8sp", "tc_bf16x2", "tc_bf16x3", "simt_f32"])
 def test_cg_result_is_the_evaluation_at_the_returned_x(gpu, path):
     """On the tensor-core paths each trial's step x_t = x + alpha s is fused into the
     first pass over x (tc_prep; the column-max pass of the integer path), which

@@ -169,3 +169,124 @@ def test_integer_path_stages(gpu, L, N, seed):
     R_gpu = digits_value(*r) / 2.0**21
     assert np.abs(R_gpu - R_exp).max() < 2.0**-21 + 2e-6
     ev.close()
+
+
+def slot192(q, l):
+    return (l // 9) * 192 + q * 9 + (l % 9)
+
+
+# Tiled storage of the sparse forward's operands (shared-memory images, swizzle
+# included); KB = KP / 128.  Index arrays map logical (row, column) to the byte.
+def sp_a_index(Npad, KP):
+    n = np.arange(Npad)[:, None]
+    col = np.arange(KP // 2)[None, :]
+    KB = KP // 128
+    r = n & 127
+    return ((((n >> 7) * KB + (col >> 6)) * 128 + r) * 64
+            + ((((col >> 4) & 3) ^ ((r >> 1) & 3)) << 4) + (col & 15))
+
+
+def sp_e_index(Npad, KP):
+    n = np.arange(Npad)[:, None]
+    b = np.arange(KP // 8)[None, :]
+    KB = KP // 128
+    return (((n >> 7) * KB + (b >> 4)) * 128 + (n & 127)) * 16 + (b & 15)
+
+
+def sp_b_index(KP, SW):
+    kr = np.arange(KP)[:, None]
+    s = np.arange(SW)[None, :]
+    KB = KP // 128
+    t, c = s // 192, s % 192
+    h, i, xx, r = c // 96, (c % 96) >> 5, c & 31, kr & 127
+    return (((((t * 2 + h) * KB + (kr >> 7)) * 3 + i) * 4096 + r * 32
+             + ((((xx >> 4) ^ (r >> 2)) & 1) << 4) + (xx & 15)))
+
+
+@pytest.mark.parametrize("L,N,seed", [(13, 50, 1), (24, 130, 2), (5, 7, 3), (40, 300, 4)])
+def test_sparse_integer_path_stages(gpu, L, N, seed):
+    """The sparse integer path (tc_i8sp): the compressed one-hot operand of the
+    forward decompresses to the one-hot in the K order l * 21 + q with valid 2:4
+    metadata (two ascending positions per group of four); the digits of W sit in
+    rows k * 21 + b and 192-slot-group columns (bit-exact); the one-hot of the
+    backward and the digits of R use the 192-slot groups.  The forward's operands
+    are read back through their tiled storage maps (each map a bijection)."""
+    import torch
+    msa = synth.generate(synth.MSAConfig("t", L, N, n_pairs=2, seed=seed))
+    w = np.random.default_rng(seed).uniform(0.2, 1.0, N).astype(np.float32)
+    x = synth.random_x(L, seed + 10, w_sd=0.05)
+    lam2 = 0.2 * (L - 1)
+    ev = Evaluator(msa, weights=w, lambda_pair=lam2, path="tc_i8sp")
+    xd = torch.from_numpy(x).cuda()
+    gd = torch.empty_like(xd)
+    ev.evaluate(xd, gd)
+    T = (L + 8) // 9
+    SW = 192 * T
+    S = (SW + 255) // 256 * 256
+    KP = (21 * L + 255) // 256 * 256
+    Npad = (N + 255) // 256 * 256
+    nsp = 20 * L + 32 - (20 * L) % 32
+    W = x[nsp:].reshape(Q, L, QP, L)[:, :, :Q, :]                       # [b,k,a,j] float32
+
+    # compressed operand and metadata -> logical one-hot in the order l * 21 + q
+    ac = fetch(ev, 9, np.uint8)[sp_a_index(Npad, KP)].astype(np.int64)
+    meta = fetch(ev, 10, np.uint8)[sp_e_index(Npad, KP)].astype(np.int64)
+    nib = np.stack([meta & 15, meta >> 4], axis=2).reshape(Npad, KP // 4)
+    i0, i1 = nib & 3, nib >> 2
+    assert np.all(i0 < i1)
+    for idx, size in ((sp_a_index(Npad, KP), Npad * KP // 2), (sp_e_index(Npad, KP), Npad * KP // 8),
+                      (sp_b_index(KP, SW), KP * SW)):
+        assert idx.size == size and np.array_equal(np.sort(idx.ravel()), np.arange(size))
+    logical = np.zeros((Npad, KP // 4, 4), dtype=np.int64)
+    rows = np.arange(Npad)[:, None]
+    grp = np.arange(KP // 4)[None, :]
+    logical[rows, grp, i0] = ac[:, 0::2]
+    logical[rows, grp, i1] += ac[:, 1::2]
+    onehot_nat = np.zeros((Npad, KP), dtype=np.int64)
+    for l in range(L):
+        onehot_nat[np.arange(N), l * Q + msa[:, l].astype(np.int64)] = 1
+    assert np.array_equal(logical.reshape(Npad, KP), onehot_nat)
+
+    # one-hot of the backward in 192-slot groups, ones slot 189
+    O1 = fetch(ev, 0, np.uint8).reshape(Npad, S)
+    O = np.zeros((Npad, S), dtype=np.uint8)
+    for n in range(N):
+        for l in range(L):
+            O[n, slot192(int(msa[n, l]), l)] = 1
+        O[n, 189] = 1
+    assert np.array_equal(O1, O)
+
+    # digits of W: rows k * 21 + b, columns s192(a, j), exact
+    cm = fetch(ev, 8, np.uint32).view(np.float32).reshape(Q, L)
+    mant, ex = np.frexp(cm.astype(np.float64))
+    e = np.where(cm == 0, 0, np.where(mant == 0.5, ex - 1, ex))
+    scale = np.ldexp(1.0, 21 - e)
+    Wq = np.clip(np.rint(W.astype(np.float64) * scale[None, None]), -2**21, 2**21 - 1)
+    bidx = sp_b_index(KP, SW)
+    d = [fetch(ev, 1 + i, np.uint8)[bidx] for i in range(3)]
+    Qgpu = digits_value(*d)
+    Qexp = np.zeros((KP, SW), dtype=np.int64)
+    rows_k = (np.arange(L)[None, :] * Q + np.arange(Q)[:, None]).reshape(-1)       # [b,k] -> k*21+b
+    cols_s = np.array([[slot192(a, j) for j in range(L)] for a in range(Q)]).reshape(-1)
+    Qexp[np.ix_(rows_k, cols_s)] = Wq.astype(np.int64).reshape(Q * L, Q * L)
+    assert np.array_equal(Qgpu, Qexp)
+
+    # R digits in 192-slot groups against the FP64 forward at the quantised W
+    V = x[:20 * L].reshape(20, L).astype(np.float64)
+    Wdeq = (Wq / scale[None, None]).reshape(Q * L, Q * L)               # rows (b,k), cols (a,j)
+    Onat = np.zeros((N, Q * L))
+    for l in range(L):
+        Onat[np.arange(N), msa[:, l].astype(np.int64) * L + l] = 1.0    # column b*L + k
+    logits = (Onat @ Wdeq).reshape(N, Q, L)                             # [n, a, j]
+    r = [fetch(ev, 4 + i, np.uint8).reshape(Npad, S) for i in range(3)]
+    R_gpu = digits_value(*r) / 2.0**21
+    R_exp = np.zeros((Npad, S))
+    for l in range(L):
+        z = logits[:, :, l].copy()
+        z[:, :20] += V[:, l][None, :]
+        z -= z.max(axis=1, keepdims=True)
+        P = np.exp(z) / np.exp(z).sum(axis=1, keepdims=True)
+        onehot = (msa[:, l][:, None] == np.arange(Q)[None, :]).astype(np.float64)
+        R_exp[:N, [slot192(a, l) for a in range(Q)]] = w[:, None] * (P - onehot)
+    assert np.abs(R_gpu - R_exp).max() < 2.0**-21 + 2e-6
+    ev.close()

@@ -28,6 +28,7 @@ TOL = {
     "tc_bf16x2": dict(f=1e-6, g=1e-5, g1=1e-5, g2=1e-5),
     "tc_bf16x3": dict(f=1e-6, g=1e-5, g1=1e-5, g2=1e-5),
     "tc_i8x3": dict(f=1e-6, g=1e-5, g1=1e-5, g2=1e-5),
+    "tc_i8sp": dict(f=1e-6, g=1e-5, g1=1e-5, g2=1e-5),
 }
 PATHS = list(TOL)
 
@@ -99,7 +100,7 @@ def test_synthetic(gpu, oracle_mod, path, name, cfg, xkind):
     assert within(e, TOL[path]), e
 
 
-@pytest.mark.parametrize("path", ["tc_bf16x2", "tc_i8x3", "simt_f32"])
+@pytest.mark.parametrize("path", ["tc_bf16x2", "tc_i8x3", "tc_i8sp", "simt_f32"])
 def test_inadmissible_x(gpu, oracle_mod, path):
     """Non-zero padding states and self blocks: g follows the CPU reference
     (2*lambda2*x there, g1 padding zero)."""
@@ -158,7 +159,7 @@ def test_reference_triple(gpu, oracle_mod):
     assert lib().destroy_cuda(ctypes.byref(ud)) == 0
 
 
-@pytest.mark.parametrize("path", ["tc_bf16x2", "tc_i8x3"])
+@pytest.mark.parametrize("path", ["tc_bf16x2", "tc_i8x3", "tc_i8sp"])
 def test_errors_and_determinism(gpu, path):
     import torch
     msa = synth.generate(synth.MSAConfig("t", 30, 200, seed=4))
