@@ -45,7 +45,7 @@ WORKLOAD = "L300_N5000"
 
 
 
-PATH_DTYPE = {"tc_bf16x2": "bf16", "tc_bf16x3": "bf16", "tc_i8x3": "int8"}
+PATH_DTYPE = {"tc_bf16x2": "bf16", "tc_bf16x3": "bf16", "tc_i8x3": "int8", "tc_i8sp": "int8"}
 PATH_ARITHMETIC = {
     "tc_bf16x2": "bf16 hi+lo split operands, f32 tensor-core accumulation, "
                  "f64 loss/regulariser reductions",
@@ -54,6 +54,8 @@ PATH_ARITHMETIC = {
     "tc_i8x3": "W and R as three 8-bit fixed-point digits (21 fractional bits, per-column "
                "power-of-two scale for W), exact s32 tensor-core accumulation, "
                "f64 loss/regulariser reductions",
+    "tc_i8sp": "as tc_i8x3 (the same exact integer sums), with the forward on 2:4-sparse "
+               "tcgen05.mma.sp over the compressed one-hot operand",
 }
 
 
@@ -80,7 +82,8 @@ def parse_args():
     p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--path", default="tc_i8x3", choices=["tc_i8x3", "tc_bf16x2", "tc_bf16x3"])
+    p.add_argument("--path", default="tc_i8sp",
+                   choices=["tc_i8sp", "tc_i8x3", "tc_bf16x2", "tc_bf16x3"])
     p.add_argument("--e2e-steps", type=int, default=50)
     p.add_argument("--plain-steps", type=int, default=20)
     p.add_argument("--compare-steps", type=int, default=300,
@@ -308,7 +311,10 @@ def reference_cuda_timing(msa, x, xd, steps, with_precision):
 def traffic_from_profiles(kernel: str, path_name: str):
     """DRAM bytes per launch of the dominant kernel from the committed ncu summary
     of the path's kernels (tc_* for the bf16 paths, i8_* for the integer path)."""
-    if path_name == "tc_i8x3":
+    if path_name == "tc_i8sp":
+        fname = "i8sp_kernels_L300_N5000.json"
+        kernel = {"tc_forward": "i8sp_forward"}.get(kernel, kernel.replace("tc_", "i8_"))
+    elif path_name == "tc_i8x3":
         fname, kernel = "i8_kernels_L300_N5000.json", kernel.replace("tc_", "i8_")
     else:
         fname = "tc_kernels_L300_N5000.json"
@@ -334,7 +340,8 @@ def run_batch(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     t0 = time.perf_counter()
-    res, _ = cb.solve_batch(msas, workers=args.batch_workers, max_iterations=250, epsilon=1e-3,
+    res, _ = cb.solve_batch(msas, workers=args.batch_workers, path=args.path, max_iterations=250,
+                            epsilon=1e-3,
                             device=local)
     torch.cuda.synchronize()
     el = max_over_ranks(world, time.perf_counter() - t0)
@@ -360,7 +367,7 @@ def run_batch(args, world, rank, local):
         "data": "synthetic", "dtype": "int8",
         "config": {"workload": "batch256: L~U[50,400], N~logU[200,20000], seeds 1000+i, "
                                "eps 1e-3 or 250 iterations",
-                   "workers": args.batch_workers, "path": "tc_i8x3"},
+                   "workers": args.batch_workers, "path": args.path},
         "wall_s": el, "solved_ok": ok, "iterations_mean": float(its.mean()),
         "plain_f32_one_at_a_time": {
             "msas_per_s_extrapolated": len(msas) / plain_total,
@@ -468,17 +475,31 @@ def main():
         # for the backward, both products O^T R and R^T O on the upper-triangle tiles
         # bf16-equivalent products per element: 2 (hi+lo), 3 (three terms); the integer
         # path does three 8-bit products at twice the bf16 rate = 1.5
-        nsplit = {"tc_bf16x3": 3, "tc_i8x3": 1.5}.get(args.path, 2)
-        T = (L + 11) // 12
-        S, Npad = 256 * T, (N + 255) // 256 * 256
-        executed = {"tc_forward": 2.0 * Npad * S * S * nsplit,
-                    "tc_backward": T * (T + 1) / 2 * 256 * 256 * 2.0 * Npad * 2 * nsplit}[dom]
+        nsplit = {"tc_bf16x3": 3, "tc_i8x3": 1.5, "tc_i8sp": 1.5}.get(args.path, 2)
+        Npad = (N + 255) // 256 * 256
+        if args.path == "tc_i8sp":
+            # forward: 192-slot groups (9 columns) as N, K = 21 L padded to 256, three
+            # 8-bit products at the 2:4-sparse rate (four times bf16): 0.75 per element;
+            # backward: the 192-slot groups padded to 256-slot tiles
+            SW = 192 * ((L + 8) // 9)
+            KP = (21 * L + 255) // 256 * 256
+            TB = (SW + 255) // 256
+            executed = {"tc_forward": 2.0 * Npad * SW * KP * 0.75,
+                        "tc_backward": TB * (TB + 1) / 2 * 256 * 256 * 2.0 * Npad * 2 * nsplit}[dom]
+        else:
+            T = (L + 11) // 12
+            S = 256 * T
+            executed = {"tc_forward": 2.0 * Npad * S * S * nsplit,
+                        "tc_backward": T * (T + 1) / 2 * 256 * 256 * 2.0 * Npad * 2 * nsplit}[dom]
         executed_tf = executed / (dom_ms / 1e3) / 1e12
 
-        other = None
-        if args.compare_steps > 0 and world == 1 and args.path != "tc_bf16x2":
-            # the split-bf16 tensor-core path on the same inputs, same timing method
-            be = cb.Evaluator(msa, weights=w, path="tc_bf16x2", device=local)
+        # the dense integer and split-bf16 tensor-core paths on the same inputs, same
+        # timing method
+        others = {}
+        for cpath in ("tc_i8x3", "tc_bf16x2"):
+            if args.compare_steps <= 0 or world != 1 or cpath == args.path:
+                continue
+            be = cb.Evaluator(msa, weights=w, path=cpath, device=local)
             gb = torch.empty_like(xd)
             for _ in range(3):
                 be.evaluate(xd, gb)
@@ -495,10 +516,10 @@ def main():
             f_b = be.result().fx
             g_b = gb.cpu().numpy()
             be.close()
-            other = {"evals_per_s": bv, "steps": args.compare_steps,
-                     "arithmetic": PATH_ARITHMETIC["tc_bf16x2"],
-                     "precision": None if args.no_precision
-                     else precision_block(msa, w, x, g_b, f_b, L)}
+            others[cpath] = {"evals_per_s": bv, "steps": args.compare_steps,
+                             "arithmetic": PATH_ARITHMETIC[cpath],
+                             "precision": None if args.no_precision
+                             else precision_block(msa, w, x, g_b, f_b, L)}
 
         plain = None
         if args.plain_steps > 0 and world == 1:
@@ -558,7 +579,8 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks,
             "plain_f32": plain,
-            "tc_bf16x2": other,
+            "tc_i8x3": others.get("tc_i8x3"),
+            "tc_bf16x2": others.get("tc_bf16x2"),
             "reference_cuda": ref_cuda,
             "precision": prec,
             "init_ms": {"weights": init_ms},

@@ -56,7 +56,7 @@ def calculate_weights(msa: np.ndarray, threshold: float = 0.8, device: int = 0) 
     return w
 
 
-def solve_batch(msas, workers: int = 8, path: str = "tc_i8x3", threshold: float = 0.8,
+def solve_batch(msas, workers: int = 8, path: str = "tc_i8sp", threshold: float = 0.8,
                 max_iterations: int = 250, epsilon: float = 0.01, contact_maps: bool = True,
                 device: int = 0, sms_per_worker: int = 0):
     """Solve many alignments to convergence concurrently (ccm_solve_batch).
@@ -87,8 +87,9 @@ def solve_batch(msas, workers: int = 8, path: str = "tc_i8x3", threshold: float 
 class Evaluator:
     """A ccm_context: the alignment, its weights and the device scratch of one path.
 
-    ``path`` is one of ``tc_i8x3`` (default: 8-bit fixed-point digits, exact integer
-    accumulation), ``tc_bf16x2``, ``tc_bf16x3``, ``simt_f32``, ``simt_f64``;
+    ``path`` is one of ``tc_i8sp`` (default: 8-bit fixed-point digits, exact integer
+    accumulation, the forward on 2:4-sparse MMAs), ``tc_i8x3`` (the same sums with a
+    dense forward), ``tc_bf16x2``, ``tc_bf16x3``, ``simt_f32``, ``simt_f64``;
     ``gradient`` is ``tied`` (the reference's g, default) or ``partial`` (true
     partial derivatives, as autograd needs them); ``max_sms`` > 0 confines the
     tensor-core kernels to that many SMs (for contexts that share one GPU).
@@ -96,7 +97,7 @@ class Evaluator:
 
     def __init__(self, msa: np.ndarray, weights: Optional[np.ndarray] = None,
                  lambda_single: float = 0.01, lambda_pair: Optional[float] = None,
-                 path: str = "tc_i8x3", device: int = 0, stream: Optional[int] = None,
+                 path: str = "tc_i8sp", device: int = 0, stream: Optional[int] = None,
                  gradient: str = "tied", max_sms: int = 0):
         self._ctx = ctypes.c_void_p(None)
         self.msa = np.ascontiguousarray(msa, dtype=np.uint8)

@@ -71,7 +71,7 @@ using namespace ccm;
 namespace {
 
 thread_local char g_last_error[512] = "";
-int g_default_path = CCM_PATH_TC_I8X3;
+int g_default_path = CCM_PATH_TC_I8SP;
 
 int set_error(int code, const char *fmt, ...) {
   va_list ap;
@@ -568,7 +568,7 @@ void ccm_options_default(ccm_options *opt, int ncol) {
   if (!opt) return;
   opt->lambda_single = 0.01f;
   opt->lambda_pair = 0.2f * (float)(ncol - 1);
-  opt->path = CCM_PATH_TC_I8X3;
+  opt->path = CCM_PATH_TC_I8SP;
   opt->device = 0;
   opt->stream = nullptr;
   opt->gradient = CCM_GRADIENT_TIED;

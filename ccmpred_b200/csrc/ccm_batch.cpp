@@ -32,7 +32,7 @@ void ccm_batch_params_default(ccm_batch_params *p) {
   p->reweighting_threshold = 0.8f;
   p->lambda_single = 0.01f;
   p->lambda_pair_factor = 0.2f;
-  p->path = CCM_PATH_TC_I8X3;
+  p->path = CCM_PATH_TC_I8SP;
   p->workers = 8;
   p->device = 0;
   p->use_apc = 1;

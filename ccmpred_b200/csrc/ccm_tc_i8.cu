@@ -154,7 +154,9 @@ __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ 
                                                       float *__restrict__ g2, I8PrepArgs args) {
   extern __shared__ __align__(16) float xrow[];  // S floats: the row in slot order
   const int L = args.L;
-  const int row = blockIdx.x;
+  // NAT: blocks in K-row order k * 21 + b, so that blocks running together fill
+  // neighbouring rows of the same stored tiles
+  const int row = NAT ? (int)(blockIdx.x % kQ) * L + (int)(blockIdx.x / kQ) : (int)blockIdx.x;
   const int b = row / L, k = row % L;
   const long long base = (long long)row * kQPad * L;
   const float two_l2 = args.g2_coef * args.lambda_pair;

@@ -161,6 +161,7 @@ int main(int argc, char **argv) {
 	if (path && strcmp(path, "tc_bf16x2") == 0) o.path = CCM_PATH_TC_BF16X2;
 	if (path && strcmp(path, "tc_bf16x3") == 0) o.path = CCM_PATH_TC_BF16X3;
 	if (path && strcmp(path, "simt_f32") == 0) o.path = CCM_PATH_SIMT_F32;
+	if (path && strcmp(path, "tc_i8x3") == 0) o.path = CCM_PATH_TC_I8X3;
 	ccm_context *ctx = NULL;
 	if (ccm_create(&ctx, msa, ncol, nrow, weights, &o) != CCM_OK) die(ccm_last_error());
 

@@ -76,7 +76,7 @@ typedef struct ccm_context ccm_context;
 typedef struct ccm_options {
 	float lambda_single; /* default 0.01 (src/ccmpred.c:222) */
 	float lambda_pair;   /* default 0.2 * (L - 1) (src/ccmpred.c:224,502-503) */
-	int path;            /* CCM_PATH_* ; default CCM_PATH_TC_I8X3 */
+	int path;            /* CCM_PATH_* ; default CCM_PATH_TC_I8SP */
 	int device;          /* CUDA device ordinal; default 0 */
 	void *stream;        /* cudaStream_t to run on, or NULL for a private stream that is
 	                        ordered with the legacy default stream */
@@ -207,7 +207,7 @@ CCM_API int ccm_calculate_weights_noalloc(const unsigned char *d_msa, int ncol, 
 /* Description of the last error on this host thread. */
 CCM_API const char *ccm_last_error(void);
 
-/* Path used by init_cuda/init_b200 (CCM_PATH_*); default CCM_PATH_TC_I8X3. */
+/* Path used by init_cuda/init_b200 (CCM_PATH_*); default CCM_PATH_TC_I8SP. */
 CCM_API void ccm_set_default_path(int path);
 
 /* ---------------------------------------------------------------- optimizer */
