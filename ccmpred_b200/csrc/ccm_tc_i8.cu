@@ -66,7 +66,8 @@ __global__ void __launch_bounds__(256) i8_colmax_kernel(const float *__restrict_
                                                         const double *__restrict__ alpha,
                                                         float *__restrict__ xt,
                                                         uint32_t *__restrict__ colmax, int L,
-                                                        long long nsp, int rows_per_block) {
+                                                        long long nsp, int rows_per_block,
+                                                        int krow_order) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int w32 = kQPad * L;
   float a = 0.0f;
@@ -82,7 +83,12 @@ __global__ void __launch_bounds__(256) i8_colmax_kernel(const float *__restrict_
   const int r1 = min(r0 + rows_per_block, kQ * L);
   float m = 0.0f;
   for (int r = r0; r < r1; ++r) {
-    const long long i = nsp + (long long)r * w32 + c;
+    // rows in the reverse of the order in which prep reads them (plain row order, or
+    // the sparse path's K-row order k * 21 + b), so that prep's first rows are the
+    // ones read last here and are still in L2
+    const int rr = kQ * L - 1 - r;
+    const int row = krow_order ? (rr % kQ) * L + rr / kQ : rr;
+    const long long i = nsp + (long long)row * w32 + c;
     float v = x[i];
     if (STEP) {
       v = fmaf(a, s[i], v);
@@ -1238,10 +1244,11 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   const dim3 cgrid((kQPad * L + 255) / 256, (kQ * L + kRows - 1) / kRows + (step ? 1 : 0));
   if (step)
     i8_colmax_kernel<true><<<cgrid, 256, 0, c->stream>>>(d_x, d_s, d_alpha, d_xt, c->d_colmax,
-                                                          L, c->nsp, kRows);
+                                                          L, c->nsp, kRows, sp ? 1 : 0);
   else
     i8_colmax_kernel<false><<<cgrid, 256, 0, c->stream>>>(d_x, nullptr, nullptr, nullptr,
-                                                           c->d_colmax, L, c->nsp, kRows);
+                                                           c->d_colmax, L, c->nsp, kRows,
+                                                           sp ? 1 : 0);
   // per-slot factors after the column maxima, 16-byte aligned for the float4 loads
   float *enc = reinterpret_cast<float *>(c->d_colmax + ((kQ * L + 3) & ~3));
   // W digit rows: S slots (dense forward) or SW slots of 192-slot groups (sparse)
