@@ -173,3 +173,26 @@ def test_errors_and_determinism(gpu, path):
     f2 = ev.evaluate(x, g)
     assert f1 == f2 and torch.equal(g, g1)   # bit-for-bit deterministic
     ev.close()
+
+
+@pytest.mark.parametrize("path", ["tc_i8sp", "tc_i8x3"])
+def test_long_alignment_against_f64_path(gpu, path):
+    """L = 700: the integer paths' prep runs the one-row-per-block kernel there (two
+    32 L-float rows no longer fit in shared memory beside the slot row); checked
+    against the FP64 CUDA-core path, itself checked against the oracle above."""
+    import torch
+    msa = synth.generate(synth.MSAConfig("t", 700, 96, n_pairs=20, seed=21))
+    N, L = msa.shape
+    w = calculate_weights(msa, 0.8)
+    x = synth.random_x(L, 22)
+    xd = torch.from_numpy(x).cuda()
+    ref = Evaluator(msa, weights=w, path="simt_f64")
+    g64 = torch.empty_like(xd, dtype=torch.float64)
+    f64 = ref.evaluate(xd.double(), g64)
+    ref.close()
+    ev = Evaluator(msa, weights=w, path=path)
+    g = torch.full_like(xd, float("nan"))
+    f = ev.evaluate(xd, g)
+    ev.close()
+    e = errors(f, g.cpu().numpy(), f64, g64.cpu().numpy(), L)
+    assert within(e, TOL[path]), e
