@@ -177,9 +177,9 @@ def test_errors_and_determinism(gpu, path):
 
 @pytest.mark.parametrize("path", ["tc_i8sp", "tc_i8x3"])
 def test_long_alignment_against_f64_path(gpu, path):
-    """L = 700: the integer paths' prep runs the one-row-per-block kernel there (two
-    32 L-float rows no longer fit in shared memory beside the slot row); checked
-    against the FP64 CUDA-core path, itself checked against the oracle above."""
+    """L = 700, a long alignment (prep stages rows of ~15k slots in shared memory, the
+    backward's slot space is ~59 pair-tile blocks, K = 14700 for the sparse forward),
+    checked against the FP64 CUDA-core path, itself checked against the oracle above."""
     import torch
     msa = synth.generate(synth.MSAConfig("t", 700, 96, n_pairs=20, seed=21))
     N, L = msa.shape
