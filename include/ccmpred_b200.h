@@ -175,10 +175,15 @@ CCM_API int ccm_profile_end(ccm_context *ctx, double *kernel_ms, int max_kernels
 CCM_API long long ccm_launch_count(const ccm_context *ctx);
 
 /* Diagnostics for tests: copy an internal device buffer of a tensor-core
- * context to host memory `dst` (`bytes` long).  which = 0: one-hot O
- * (Npad x S bf16); 1..3: Wperm split terms (S x S bf16); 4..6: R split terms
- * (Npad x S bf16); 7: single-field data gradient (20 L float).  With dst ==
- * NULL returns the buffer size in bytes; otherwise 0 or a negative status. */
+ * context to host memory `dst` (`bytes` long).  Split-bf16 paths: which = 0:
+ * one-hot O (Npad x S bf16); 1..3: Wperm split terms (S x S bf16); 4..6: R split
+ * terms (Npad x S bf16); 7: single-field data gradient (20 L float).  Integer
+ * paths: 0: one-hot (Npad x S bytes, values 1); 1..3: digits of W (S x S bytes;
+ * CCM_PATH_TC_I8SP: KP x SW bytes in the forward's tiled storage); 4..6: digits
+ * of R (Npad x S bytes); 7: as above; 8: column maxima of |W| (21 L float bits);
+ * CCM_PATH_TC_I8SP only: 9: compressed one-hot (Npad x KP/2 bytes, tiled),
+ * 10: its 2:4 metadata (Npad x KP/8 bytes, tiled).  With dst == NULL returns the
+ * buffer size in bytes; otherwise 0 or a negative status. */
 CCM_API long long ccm_debug_copy(ccm_context *ctx, int which, void *dst, long long bytes);
 
 /* Allocation-free sequence reweighting.  No counterpart in the reference.

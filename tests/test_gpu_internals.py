@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 from ccmpred_b200 import Evaluator, lib, synth
+from sparse_layout import slot192, sp_a_index, sp_b_index, sp_e_index
 
 pytestmark = pytest.mark.gpu
 
@@ -169,38 +170,6 @@ def test_integer_path_stages(gpu, L, N, seed):
     R_gpu = digits_value(*r) / 2.0**21
     assert np.abs(R_gpu - R_exp).max() < 2.0**-21 + 2e-6
     ev.close()
-
-
-def slot192(q, l):
-    return (l // 9) * 192 + q * 9 + (l % 9)
-
-
-# Tiled storage of the sparse forward's operands (shared-memory images, swizzle
-# included); KB = KP / 128.  Index arrays map logical (row, column) to the byte.
-def sp_a_index(Npad, KP):
-    n = np.arange(Npad)[:, None]
-    col = np.arange(KP // 2)[None, :]
-    KB = KP // 128
-    r = n & 127
-    return ((((n >> 7) * KB + (col >> 6)) * 128 + r) * 64
-            + ((((col >> 4) & 3) ^ ((r >> 1) & 3)) << 4) + (col & 15))
-
-
-def sp_e_index(Npad, KP):
-    n = np.arange(Npad)[:, None]
-    b = np.arange(KP // 8)[None, :]
-    KB = KP // 128
-    return (((n >> 7) * KB + (b >> 4)) * 128 + (n & 127)) * 16 + (b & 15)
-
-
-def sp_b_index(KP, SW):
-    kr = np.arange(KP)[:, None]
-    s = np.arange(SW)[None, :]
-    KB = KP // 128
-    t, c = s // 192, s % 192
-    h, i, xx, r = c // 96, (c % 96) >> 5, c & 31, kr & 127
-    return (((((t * 2 + h) * KB + (kr >> 7)) * 3 + i) * 4096 + r * 32
-             + ((((xx >> 4) ^ (r >> 2)) & 1) << 4) + (xx & 15)))
 
 
 @pytest.mark.parametrize("L,N,seed", [(13, 50, 1), (24, 130, 2), (5, 7, 3), (40, 300, 4)])
