@@ -314,15 +314,20 @@ struct I8FwdSmem {
 //          halves), lse = M + log S;
 //   C:     P = e * exp(m - M) / S, R = w (P - onehot) as its three digits.
 // G: the slot groups of the tile (one group = one tile, G::kSlots columns, half
-// of them per warp).
-template <class G, int H>
+// of them per warp).  REGS: the merged logits leave both accumulators during the
+// merge -- the half's first 32-column chunk into a TMEM stash that no MMA writes
+// (t_stash), the other chunks into registers -- and the arrival on `lo_bar` after
+// the merge then releases both accumulators, so that the next tile's MMAs run
+// during passes B and C.
+template <class G, int H, bool REGS = false>
 __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint32_t t_hi,
                                                      uint32_t t_lo, const float *tab_scale,
                                                      const float *tab_v, float *xbuf, int q,
                                                      int lane, int n, int t, long long part,
-                                                     uint32_t lo_bar) {
+                                                     uint32_t lo_bar, uint32_t t_stash = 0) {
   constexpr int kGroupCols = G::kCols, kGroupUsed = G::kUsed;
   constexpr int kChunks = G::kSlots / 64;  // 32-column chunks per half
+  uint32_t zr[REGS ? (kChunks - 1) * 32 : 1];  // REGS: chunks 1.. of the half
   const int L = args.L;
   const int j0 = t * kGroupCols;
   const bool live = n < args.N;
@@ -339,8 +344,35 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
 #pragma unroll
   for (int jj = 0; jj < kGroupCols; ++jj) { mx[jj] = -INFINITY; tg[jj] = 0.0f; se[jj] = 0.0f; }
   // merge + maxima
+  if constexpr (REGS) {
+    // 16-column steps: steps 0 and 1 fill the stash, the others the registers
+    uint32_t st[32];
 #pragma unroll
-  for (int c = 0; c < kChunks; ++c) {
+    for (int c = 0; c < 2 * kChunks; ++c) {
+      const int cc = 2 * kChunks * H + c;
+      uint32_t vh[16], vl[16];
+      __syncwarp();
+      tmem_ld16(t_hi + cc * 16, vh);
+      tmem_ld16(t_lo + cc * 16, vl);
+      tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int col = cc * 16 + i;
+        const long long qs = (long long)(int)vh[i] * 16384 + (long long)(int)vl[i];
+        const float z = fmaf(__ll2float_rn(qs), tab_scale[col], tab_v[col]);
+        if (c < 2) st[c * 16 + i] = __float_as_uint(z);
+        else zr[(c - 2) * 16 + i] = __float_as_uint(z);
+        if (col < kGroupUsed) {
+          const int a = col / kGroupCols, jj = col % kGroupCols;
+          mx[jj] = fmaxf(mx[jj], z);
+          if (xr[jj] == a) tg[jj] = z;
+        }
+      }
+      if (c == 1) tmem_st32(t_stash, st);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < (REGS ? 0 : kChunks); ++c) {
     const int cc = kChunks * H + c;
     uint32_t vh[32], vl[32];
     __syncwarp();
@@ -364,14 +396,30 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
   tmem_wait_st();
   tc_fence_before();
   __syncwarp();
-  if (lane == 0) mbar_arrive_cluster(lo_bar);  // the next tile's low phase may start
+  // the next tile's low phase (REGS: its MMAs) may start
+  if (lane == 0) mbar_arrive_cluster(lo_bar);
   // B: e = exp(z - m), sum
 #pragma unroll
   for (int c = 0; c < kChunks; ++c) {
     const int cc = kChunks * H + c;
+    if constexpr (REGS) {
+      if (c > 0) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          const int col = cc * 32 + i;
+          if (col < kGroupUsed) {
+            const int jj = col % kGroupCols;
+            const float e = expf(__uint_as_float(zr[(c - 1) * 32 + i]) - mx[jj]);
+            se[jj] += e;
+            zr[(c - 1) * 32 + i] = __float_as_uint(e);
+          }
+        }
+        continue;
+      }
+    }
     uint32_t v[32];
     __syncwarp();
-    tmem_ld32(t_hi + cc * 32, v);
+    tmem_ld32(REGS ? t_stash : t_hi + cc * 32, v);
     tmem_wait_ld();
 #pragma unroll
     for (int i = 0; i < 32; ++i) {
@@ -383,7 +431,7 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
         v[i] = __float_as_uint(e);
       }
     }
-    tmem_st32(t_hi + cc * 32, v);
+    tmem_st32(REGS ? t_stash : t_hi + cc * 32, v);
   }
   float *mine = xbuf + (H * kI8BM + row) * (2 * kGroupCols);
   const float *other = xbuf + ((1 - H) * kI8BM + row) * (2 * kGroupCols);
@@ -414,10 +462,16 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
 #pragma unroll
   for (int c = 0; c < kChunks; ++c) {
     const int cc = kChunks * H + c;
-    uint32_t v[32];
-    __syncwarp();
-    tmem_ld32(t_hi + cc * 32, v);
-    tmem_wait_ld();
+    uint32_t vbuf[32];
+    if (!REGS || c == 0) {
+      __syncwarp();
+      tmem_ld32(REGS ? t_stash : t_hi + cc * 32, vbuf);
+      tmem_wait_ld();
+    }
+    auto v = [&](int i) -> uint32_t {
+      if constexpr (REGS) return c == 0 ? vbuf[i] : zr[(c - 1) * 32 + i];
+      else return vbuf[i];
+    };
     uint32_t w0[8], w1[8], w2[8];
 #pragma unroll
     for (int e4 = 0; e4 < 8; ++e4) {
@@ -429,7 +483,7 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
         float t = 0.0f;
         if (col < kGroupUsed) {
           const int a = col / kGroupCols, jj = col % kGroupCols;
-          t = fmaf(__uint_as_float(v[i]), cw[jj], xr[jj] == a ? -won : 0.0f);
+          t = fmaf(__uint_as_float(v(i)), cw[jj], xr[jj] == a ? -won : 0.0f);
         }
         // |R| < 1: only the top of the range needs the clamp (P rounding to 1)
         qv[e] = min(__float2int_rn(t), (1 << kI8FracBits) - 1);
@@ -716,21 +770,28 @@ __global__ void i8sp_onehot_kernel(const uint8_t *__restrict__ msa, uint32_t *__
 // execute in order; two metadata slots alternate), and B -- the digits of W with
 // rows in the K order k' -- MN-major, 96 columns per CTA as three 32-byte
 // swizzled atoms of 128 K rows.  Each of these is one TMA box of the tiled
-// storage above (no TMA swizzle: the images are stored swizzled).  TMEM: hi = [0, 192), lo = [256, 448), metadata
+// storage above (no TMA swizzle: the images are stored swizzled).
+// One pass per tile: a stage holds everything one block of 128 logical K needs
+// for the three digit products (A x1, A x128, B d0..d2, E; 54 KB), so the one-hot
+// operand and its metadata cross L2 once per tile, not once per digit phase; the
+// kernel is bound by this L2 -> shared-memory operand stream.  The epilogue takes
+// the merged logits out of both accumulators during its merge pass (into TMEM
+// columns [192, 256) and registers) and releases them at once, so the next tile's
+// MMAs overlap the softmax and the R digits.
+// TMEM: hi = [0, 192), epilogue stash = [192, 256), lo = [256, 448), metadata
 // slots at 448 and 452.
 constexpr int kSpBN = Groups192::kSlots, kSpBK = 128;
 
 struct I8SpSmem {
-  static constexpr int kStages = 4;
+  static constexpr int kStages = 3;
   static constexpr int kA = kI8BM * kSpBK / 2;  // 8 KB
   static constexpr int kAtom = kSpBK * 32;      // 4 KB: 128 K rows x 32 columns
   static constexpr int kB = 3 * kAtom;          // 12 KB: 96 columns
   static constexpr int kE = kI8BM * kSpBK / 8;  // 2 KB
-  // low phase (one K block):   A x128 | A x1 | B d1 | B d2 | E
-  // high phase (two K blocks): A x1 (kb) | A x1 (kb+1) | B d0 (kb) | B d0 (kb+1) | E (kb) | E (kb+1)
-  static constexpr int kOffA0 = 0, kOffA1 = kA, kOffB0 = 2 * kA, kOffB1 = 2 * kA + kB;
-  static constexpr int kOffE0 = 2 * kA + 2 * kB, kOffE1 = kOffE0 + kE;
-  static constexpr int kStage = kOffE1 + kE;
+  // one K block of 128 logical K for all three digit products:
+  // A x1 | A x128 | B d0 | B d1 | B d2 | E
+  static constexpr int kOffA1 = 0, kOffA128 = kA, kOffB = 2 * kA, kOffE = 2 * kA + 3 * kB;
+  static constexpr int kStage = kOffE + kE;
   static constexpr int kBarOff = kStages * kStage;
   static constexpr int kTabOff = kBarOff + 256;  // per tile: scale[192], V[192]
   static constexpr int kXOff = kTabOff + 2 * kSpBN * 4;
@@ -747,9 +808,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + SM::kBarOff);
   uint64_t *empty = full + kStages;
   uint64_t *acc_full = empty + kStages;
-  uint64_t *lo_empty = acc_full + 1;
-  uint64_t *hi_empty = lo_empty + 1;
-  uint64_t *drain = hi_empty + 1;
+  uint64_t *acc_empty = acc_full + 1;
+  uint64_t *drain = acc_empty + 1;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
   int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
   float *tab_scale = reinterpret_cast<float *>(smem + SM::kTabOff);
@@ -760,13 +820,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
   const uint32_t rank = cluster_ctarank();
   const int pair = blockIdx.x >> 1, npairs = gridDim.x >> 1;
   const int n_tiles = args.m_tiles * args.T;
-  const int k_blocks = args.KP / kSpBK;  // even
+  const int k_blocks = args.KP / kSpBK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
     mbar_init(acc_full, 1);
-    mbar_init(lo_empty, 16);
-    mbar_init(hi_empty, 16);
+    mbar_init(acc_empty, 16);
     mbar_init(drain, 1);
     *abort_flag = 0;
     fence_mbar_init();
@@ -782,7 +841,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
   cluster_sync();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
+  // TMEM: hi [0, 192), the epilogue's stash [192, 256), lo [256, 448), metadata 448 / 452
   const uint32_t t_hi = tmem_base, t_lo = tmem_base + 256, t_e = tmem_base + 448;
+  const uint32_t t_stash = tmem_base + kSpBN;
 
   if (warp == 0) {
     if (lane == 0) {
@@ -793,36 +854,23 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
         const int m = tile % args.m_tiles, t = tile / args.m_tiles;
         // tile rows of the tiled operands (256-byte rows): A 32, E 8, B 48 per K block
         const int m128 = 2 * m + (int)rank, tb = 2 * t + (int)rank;
-        for (int phase = 0; phase < 2 && ok; ++phase) {  // 0: low digits, 1: high digit
-          for (int kb = 0; kb < k_blocks; kb += (phase == 0 ? 1 : 2), ++it) {
-            const int stage = it % kStages;
-            const uint32_t round = it / kStages;
-            if (!mbar_wait(&empty[stage], (round & 1) ^ 1)) {
-              i8_record_error(args.status, kErrFwdTimeout, abort_flag);
-              ok = false;
-              break;
-            }
-            uint8_t *st = smem + stage * SM::kStage;
-            const uint32_t fb = mapa_shared(smem_u32(&full[stage]), 0);
-            if (phase == 0) {
-              if (rank == 0) mbar_arrive_expect_tx(&full[stage], 2 * (2 * SM::kA + 2 * SM::kB + SM::kE));
-              tma_load_2d_pair(st + SM::kOffA0, &maps.a128, fb, 0, (m128 * k_blocks + kb) * 32);
-              tma_load_2d_pair(st + SM::kOffA1, &maps.a1, fb, 0, (m128 * k_blocks + kb) * 32);
-              tma_load_2d_pair(st + SM::kOffB0, &maps.b[1], fb, 0, (tb * k_blocks + kb) * 48);
-              tma_load_2d_pair(st + SM::kOffB1, &maps.b[2], fb, 0, (tb * k_blocks + kb) * 48);
-              tma_load_2d_pair(st + SM::kOffE0, &maps.e, fb, 0, (m128 * k_blocks + kb) * 8);
-            } else {
-              if (rank == 0) mbar_arrive_expect_tx(&full[stage], 2 * SM::kStage);
-              for (int sub = 0; sub < 2; ++sub) {
-                const int k2 = kb + sub;
-                tma_load_2d_pair(st + sub * SM::kA, &maps.a1, fb, 0, (m128 * k_blocks + k2) * 32);
-                tma_load_2d_pair(st + SM::kOffB0 + sub * SM::kB, &maps.b[0], fb, 0,
-                                 (tb * k_blocks + k2) * 48);
-                tma_load_2d_pair(st + SM::kOffE0 + sub * SM::kE, &maps.e, fb, 0,
-                                 (m128 * k_blocks + k2) * 8);
-              }
-            }
+        for (int kb = 0; kb < k_blocks; ++kb, ++it) {
+          const int stage = it % kStages;
+          const uint32_t round = it / kStages;
+          if (!mbar_wait(&empty[stage], (round & 1) ^ 1)) {
+            i8_record_error(args.status, kErrFwdTimeout, abort_flag);
+            ok = false;
+            break;
           }
+          uint8_t *st = smem + stage * SM::kStage;
+          const uint32_t fb = mapa_shared(smem_u32(&full[stage]), 0);
+          const int ya = (m128 * k_blocks + kb) * 32, yb = (tb * k_blocks + kb) * 48;
+          if (rank == 0) mbar_arrive_expect_tx(&full[stage], 2 * SM::kStage);
+          tma_load_2d_pair(st + SM::kOffA1, &maps.a1, fb, 0, ya);
+          tma_load_2d_pair(st + SM::kOffA128, &maps.a128, fb, 0, ya);
+          for (int i = 0; i < 3; ++i)
+            tma_load_2d_pair(st + SM::kOffB + i * SM::kB, &maps.b[i], fb, 0, yb);
+          tma_load_2d_pair(st + SM::kOffE, &maps.e, fb, 0, (m128 * k_blocks + kb) * 8);
         }
       }
       const uint32_t issued = it;
@@ -844,52 +892,37 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
       bool ok = true;
       for (int tile = pair; tile < n_tiles && ok && !i8_aborted(abort_flag);
            tile += npairs, ++local) {
-        const uint32_t wpar = (local & 1) ^ 1;
-        for (int phase = 0; phase < 2 && ok; ++phase) {
-          if (!mbar_wait(phase == 0 ? lo_empty : hi_empty, wpar)) {
+        // both accumulators free: the previous tile's epilogue finished its merge
+        if (!mbar_wait(acc_empty, (local & 1) ^ 1)) {
+          i8_record_error(args.status, kErrFwdTimeout, abort_flag);
+          break;
+        }
+        tc_fence_after();
+        for (int kb = 0; kb < k_blocks; ++kb, ++it) {
+          const int stage = it % kStages;
+          const uint32_t round = it / kStages;
+          if (!mbar_wait(&full[stage], round & 1)) {
             i8_record_error(args.status, kErrFwdTimeout, abort_flag);
             ok = false;
             break;
           }
           tc_fence_after();
-          for (int kb = 0; kb < k_blocks; kb += (phase == 0 ? 1 : 2), ++it) {
-            const int stage = it % kStages;
-            const uint32_t round = it / kStages;
-            if (!mbar_wait(&full[stage], round & 1)) {
-              i8_record_error(args.status, kErrFwdTimeout, abort_flag);
-              ok = false;
-              break;
-            }
-            tc_fence_after();
-            const uint32_t s0 = smem_u32(smem + stage * SM::kStage);
-            if (phase == 0) {
-              const uint32_t te = t_e + 4 * (ecopies++ & 1);
-              tmem_cp_pair_128x128b(te, sdesc_noswz(s0 + SM::kOffE0, 2048, 128));
+          const uint32_t s0 = smem_u32(smem + stage * SM::kStage);
+          const uint32_t te = t_e + 4 * (ecopies++ & 1);
+          tmem_cp_pair_128x128b(te, sdesc_noswz(s0 + SM::kOffE, 2048, 128));
 #pragma unroll
-              for (int k = 0; k < 2; ++k) {
-                const uint64_t a128 = sdesc_sw64(s0 + SM::kOffA0 + k * 32, 16, 512);
-                const uint64_t a1 = sdesc_sw64(s0 + SM::kOffA1 + k * 32, 16, 512);
-                const uint64_t bA = sdesc_sw32(s0 + SM::kOffB0 + k * 2048, SM::kAtom, 256);
-                const uint64_t bB = sdesc_sw32(s0 + SM::kOffB1 + k * 2048, SM::kAtom, 256);
-                umma_i8sp_pair(t_lo, a128, bA, idesc, te + 2 * k, (kb | k) != 0);
-                umma_i8sp_pair(t_lo, a1, bB, idesc, te + 2 * k, 1);
-              }
-            } else {
-#pragma unroll
-              for (int sub = 0; sub < 2; ++sub) {
-                const uint32_t te = t_e + 4 * (ecopies++ & 1);
-                tmem_cp_pair_128x128b(te, sdesc_noswz(s0 + SM::kOffE0 + sub * SM::kE, 2048, 128));
-#pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                  const uint64_t a1 = sdesc_sw64(s0 + sub * SM::kA + k * 32, 16, 512);
-                  const uint64_t b0 =
-                      sdesc_sw32(s0 + SM::kOffB0 + sub * SM::kB + k * 2048, SM::kAtom, 256);
-                  umma_i8sp_pair(t_hi, a1, b0, idesc, te + 2 * k, (kb | sub | k) != 0);
-                }
-              }
-            }
-            umma_commit_pair(&empty[stage], 0x3);
+          for (int k = 0; k < 2; ++k) {
+            const uint64_t a1 = sdesc_sw64(s0 + SM::kOffA1 + k * 32, 16, 512);
+            const uint64_t a128 = sdesc_sw64(s0 + SM::kOffA128 + k * 32, 16, 512);
+            const uint64_t b0 = sdesc_sw32(s0 + SM::kOffB + k * 2048, SM::kAtom, 256);
+            const uint64_t b1 = sdesc_sw32(s0 + SM::kOffB + SM::kB + k * 2048, SM::kAtom, 256);
+            const uint64_t b2 = sdesc_sw32(s0 + SM::kOffB + 2 * SM::kB + k * 2048, SM::kAtom, 256);
+            const uint32_t first = (kb | k) != 0;
+            umma_i8sp_pair(t_hi, a1, b0, idesc, te + 2 * k, first);    // O1 x d0
+            umma_i8sp_pair(t_lo, a128, b1, idesc, te + 2 * k, first);  // O128 x d1
+            umma_i8sp_pair(t_lo, a1, b2, idesc, te + 2 * k, 1);        // O1 x d2
           }
+          umma_commit_pair(&empty[stage], 0x3);
         }
         if (ok) umma_commit_pair(acc_full, 0x3);
       }
@@ -902,8 +935,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
     const int half = (warp - 2) >> 2;
     const int ethr = threadIdx.x - 64;
     const int L = args.L;
-    const uint32_t lo_bar = mapa_shared(smem_u32(lo_empty), 0);
-    const uint32_t hi_bar = mapa_shared(smem_u32(hi_empty), 0);
+    const uint32_t empty_bar = mapa_shared(smem_u32(acc_empty), 0);
     int local = 0;
     for (int tile = pair; tile < n_tiles; tile += npairs, ++local) {
       if (named_bar_or(1, 256, i8_aborted(abort_flag))) break;
@@ -931,15 +963,15 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
       tc_fence_after();
       const uint32_t lq = (uint32_t)(q * 32) << 16;
       const long long part = (long long)tile * 2 + rank;
+      // both accumulators are released inside, right after the merge
       if (half == 0)
-        i8_fwd_epilogue_tile<Groups192, 0>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v, xbuf, q,
-                                           lane, n, t, part, lo_bar);
+        i8_fwd_epilogue_tile<Groups192, 0, true>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v,
+                                                 xbuf, q, lane, n, t, part, empty_bar,
+                                                 t_stash + lq);
       else
-        i8_fwd_epilogue_tile<Groups192, 1>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v, xbuf, q,
-                                           lane, n, t, part, lo_bar);
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive_cluster(hi_bar);
+        i8_fwd_epilogue_tile<Groups192, 1, true>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v,
+                                                 xbuf, q, lane, n, t, part, empty_bar,
+                                                 t_stash + 32 + lq);
     }
   }
 
