@@ -13,7 +13,7 @@
  *   -A          disable average product correction
  *   -R          re-normalise the output matrix to [0,1]
  *   -d DEVICE   CUDA device (default 0)
- *   -t THREADS  accepted for compatibility; this build evaluates on the GPU
+ *   -t THREADS  accepted for compatibility; this program evaluates on the GPU
  * The evaluation, the weights and the optimizer run on the GPU; the output
  * matrix is the APC-corrected Frobenius norm map written with "%.20e\t".
  */
@@ -109,7 +109,7 @@ int main(int argc, char **argv) {
 	printf("                  |_|              \n\n");
 
 	int ndev = ccm_device_count();
-	if (ndev == 0) die("No CUDA devices available; this build evaluates on the GPU");
+	if (ndev == 0) die("No CUDA devices available; this program evaluates on the GPU");
 	if (device < 0 || device >= ndev) {
 		printf("Error: %d is not a valid device number. Please choose a number between 0 and %d\n",
 		       device, ndev - 1);
