@@ -92,13 +92,15 @@ class Evaluator:
     dense forward), ``tc_bf16x2``, ``tc_bf16x3``, ``simt_f32``, ``simt_f64``;
     ``gradient`` is ``tied`` (the reference's g, default) or ``partial`` (true
     partial derivatives, as autograd needs them); ``max_sms`` > 0 confines the
-    tensor-core kernels to that many SMs (for contexts that share one GPU).
+    tensor-core kernels to that many SMs (for contexts that share one GPU);
+    ``mem_limit`` > 0 caps the context's device memory (bytes), beyond which
+    creation or the optimizer fails with CCM_ERR_NOMEM.
     """
 
     def __init__(self, msa: np.ndarray, weights: Optional[np.ndarray] = None,
                  lambda_single: float = 0.01, lambda_pair: Optional[float] = None,
                  path: str = "tc_i8sp", device: int = 0, stream: Optional[int] = None,
-                 gradient: str = "tied", max_sms: int = 0):
+                 gradient: str = "tied", max_sms: int = 0, mem_limit: int = 0):
         self._ctx = ctypes.c_void_p(None)
         self.msa = np.ascontiguousarray(msa, dtype=np.uint8)
         self.N, self.L = self.msa.shape
@@ -119,6 +121,7 @@ class Evaluator:
         opt.stream = stream
         opt.gradient = _lib.GRADIENTS[gradient]
         opt.max_sms = max_sms
+        opt.mem_limit = mem_limit
         self.gradient = gradient
         wptr = None
         if weights is not None:

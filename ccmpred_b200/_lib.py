@@ -38,7 +38,8 @@ GRADIENTS = {"tied": GRADIENT_TIED, "partial": GRADIENT_PARTIAL}
 class CcmOptions(ctypes.Structure):
     _fields_ = [("lambda_single", ctypes.c_float), ("lambda_pair", ctypes.c_float),
                 ("path", ctypes.c_int), ("device", ctypes.c_int), ("stream", ctypes.c_void_p),
-                ("gradient", ctypes.c_int), ("max_sms", ctypes.c_int)]
+                ("gradient", ctypes.c_int), ("max_sms", ctypes.c_int),
+                ("mem_limit", ctypes.c_size_t)]
 
 
 class CcmResult(ctypes.Structure):
@@ -127,6 +128,7 @@ SIGNATURES = {
     "ccm_profile_end": (ctypes.c_int, [_vp, _f64p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_int)]),
     "ccm_launch_count": (ctypes.c_longlong, [_vp]),
+    "ccm_debug_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_longlong]),
     "ccm_set_default_path": (None, [ctypes.c_int]),
     "ccm_cg_params_default": (None, [ctypes.POINTER(CcmCgParams)]),
     "ccm_conjugrad_gpu": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, ctypes.POINTER(CcmCgParams),

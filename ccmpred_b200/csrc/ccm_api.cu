@@ -1,6 +1,7 @@
 // C ABI of libccmpred_b200.so: context lifecycle, evaluation dispatch and the
 // reference-compatible backend triples.  See include/ccmpred_b200.h.
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -341,6 +342,8 @@ void free_all(ccm_context *c) {
     std::free(c->prof_events);
   }
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  // released by CUDA once the stream-ordered frees above have run
+  if (c->own_pool && c->pool) cudaMemPoolDestroy(c->pool);
 }
 
 int check_status(ccm_context *c) {
@@ -466,6 +469,21 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
     return set_error(CCM_ERR_INVALID, "ccm_create: unknown gradient mode %d", o.gradient);
   for (long long i = 0; i < (long long)ncol * nrow; ++i)
     if (msa[i] > 20) return set_error(CCM_ERR_INVALID, "ccm_create: MSA state %d > 20 at %lld", msa[i], i);
+  // the integer paths encode R = w (P - onehot) with 21 fractional bits below a
+  // power-of-two scale 2^eR >= max |w|
+  float wmax = 1.0f;
+  if (weights)
+    for (int i = 0; i < nrow; ++i) {
+      if (!std::isfinite(weights[i]))
+        return set_error(CCM_ERR_INVALID, "ccm_create: weight %d is not finite", i);
+      wmax = std::max(wmax, std::fabs(weights[i]));
+    }
+  int r_exp = 0;
+  if (wmax > 1.0f) {
+    (void)std::frexp(wmax, &r_exp);                   // wmax = m 2^r_exp, m in [0.5, 1)
+    if (std::ldexp(1.0f, r_exp - 1) == wmax) --r_exp;  // an exact power of two
+    if (r_exp > 100) return set_error(CCM_ERR_INVALID, "ccm_create: weight %g too large", wmax);
+  }
   // the coupling block has 21*32*L^2 entries; keep every index in 32-bit range of int callers
   if (nvar_padded_of(ncol) > 0x7fffffffLL)
     return set_error(CCM_ERR_INVALID, "ccm_create: L=%d exceeds the int nvar of the reference ABI", ncol);
@@ -481,8 +499,26 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
   int rc = ensure_configured(o.device);
   if (rc != CCM_OK) return rc;
 
+  bool own_pool = false;
+  if (o.mem_limit > 0 && !pool) {
+    // a private pool whose maximum size is the cap (rounded up to 2 MiB)
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = o.device;
+    props.maxSize = (o.mem_limit + (2u << 20) - 1) & ~(size_t)((2u << 20) - 1);
+    cudaError_t e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess)
+      return set_error(CCM_ERR_CUDA, "ccm_create: memory pool of %zu bytes: %s", props.maxSize,
+                       cudaGetErrorString(e));
+    own_pool = true;
+  }
   ccm_context *c = new ccm_context();
   c->pool = pool;
+  c->own_pool = own_pool;
+  c->r_exp = r_exp;
   c->device = o.device;
   c->num_sms = prop.multiProcessorCount;
   if (tc_path) {
@@ -494,6 +530,7 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
     if (e == cudaSuccess)
       e = i8 ? i8_backward_max_pairs(&c->bwd_pairs) : tc_backward_max_pairs(ns, &c->bwd_pairs);
     if (e != cudaSuccess || c->fwd_pairs < 1 || c->bwd_pairs < 1) {
+      if (c->own_pool) cudaMemPoolDestroy(c->pool);
       delete c;
       return set_error(CCM_ERR_CUDA, "tc_forward cluster occupancy: %s", cudaGetErrorString(e));
     }
@@ -519,10 +556,19 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
     // a blocking stream: ordered with the legacy default stream, on which callers
     // (and torch by default) produce x and consume g
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault);
-    if (e != cudaSuccess) { delete c; return set_error(CCM_ERR_CUDA, "stream: %s", cudaGetErrorString(e)); }
+    if (e != cudaSuccess) {
+      if (c->own_pool) cudaMemPoolDestroy(c->pool);
+      delete c;
+      return set_error(CCM_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
+    }
     c->own_stream = true;
   }
-  auto fail = [&](int code) { free_all(c); delete c; return code; };
+  auto fail = [&](int code) {
+    free_all(c);
+    delete c;
+    (void)cudaGetLastError();  // a failed allocation must not surface in a later launch check
+    return code;
+  };
 #define CCM_CTX_TRY(expr)                                                                    \
   do {                                                                                       \
     cudaError_t _e = (expr);                                                                 \
@@ -573,6 +619,7 @@ void ccm_options_default(ccm_options *opt, int ncol) {
   opt->stream = nullptr;
   opt->gradient = CCM_GRADIENT_TIED;
   opt->max_sms = 0;
+  opt->mem_limit = 0;
 }
 
 int ccm_create(ccm_context **out, const unsigned char *msa, int ncol, int nrow,
@@ -704,6 +751,12 @@ int ccm_profile_end(ccm_context *c, double *kernel_ms, int max_kernels, int *n_k
 }
 
 long long ccm_launch_count(const ccm_context *c) { return c ? c->launches : -1; }
+
+int ccm_debug_set_wait_limit(ccm_context *c, long long cycles) {
+  if (!c || cycles < 0) return set_error(CCM_ERR_INVALID, "ccm_debug_set_wait_limit: invalid arguments");
+  c->acc_wait_cycles = cycles;
+  return CCM_OK;
+}
 
 const ccm_result *ccm_result_device(const ccm_context *c) { return c ? c->d_out : nullptr; }
 

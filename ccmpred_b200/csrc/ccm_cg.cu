@@ -281,6 +281,7 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
   if (!st.h_alpha || !st.h_out) chk(cudaErrorMemoryAllocation);
   if (e != cudaSuccess) {
     free_state(st);
+    (void)cudaGetLastError();  // a failed allocation must not surface in a later launch check
     return set_last_error(e == cudaErrorMemoryAllocation ? CCM_ERR_NOMEM : CCM_ERR_CUDA,
                           "ccm_conjugrad_gpu: %s", cudaGetErrorString(e));
   }

@@ -67,6 +67,13 @@ struct I8FwdArgs {
   int *status;
   int L, N, S, T, Npad, m_tiles;
   int KP;  // sparse forward: logical K (a multiple of 256)
+  // digits of R: R * r_enc with r_enc = 2^(21 - eR), eR = ceil(log2 max |w|) for
+  // weights above 1, else 0, so that |R| <= max |w| stays within 21 bits
+  float r_enc;
+  // > 0: instead of waiting for a finished accumulator, the epilogue waits this
+  // many clock cycles on a barrier that nothing arrives on, so that the wait runs
+  // out and the kernel takes its timeout path (a test of that path; 0 normally)
+  long long acc_wait_cycles;
 };
 
 struct PrepArgs {
@@ -101,6 +108,7 @@ struct BwdArgs {
   int *status;
   int n_tiles, L, S, Npad;
   float lambda_pair;
+  float r_dec;  // integer path: 2^(eR - 21), the inverse of I8FwdArgs::r_enc
 };
 
 struct FinalizeArgs {
@@ -182,6 +190,7 @@ struct ccm_context {
   int bwd_pairs = 74;             // resident CTA pairs of tc_backward
   cudaStream_t stream = nullptr;
   cudaMemPool_t pool = nullptr;   // device memory pool, or null for the device's default pool
+  bool own_pool = false;          // pool created for ccm_options.mem_limit (destroyed with the context)
   bool own_stream = false;
   int path = CCM_PATH_TC_BF16X2;
   int nsplit = 2;
@@ -189,6 +198,8 @@ struct ccm_context {
 
   int L = 0, N = 0;
   long long nsingle = 0, nsp = 0, nvarp = 0;
+  int r_exp = 0;                   // eR of the integer path's R digits (weights above 1)
+  long long acc_wait_cycles = 0;   // ccm_debug_set_wait_limit (0: default budget)
   float lambda_single = 0.01f, lambda_pair = 0.0f;
 
   uint8_t *d_msa = nullptr;       // N x L

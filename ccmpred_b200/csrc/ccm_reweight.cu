@@ -8,7 +8,6 @@
 // visits the diagonal once and increments w[i] twice).  Counts are integers,
 // so the order of the atomic additions does not matter.
 #include <cstdio>
-#include <mutex>
 
 #include <cuda_runtime.h>
 
@@ -166,20 +165,19 @@ __global__ void __launch_bounds__(256) rw_count_bytes_kernel(const uint8_t *__re
 
   for (int w0 = 0; w0 < words; w0 += kRwChunk) {
     __syncthreads();
-    for (int e = threadIdx.x; e < kRwTile * kRwChunk; e += blockDim.x) {
-      const int r = e / kRwChunk, wd = e % kRwChunk;
-      const int ia = i0 + r, jb = j0 + r, k0 = (w0 + wd) * 4;
-      uint32_t wa = 0, wb = 0;
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const int k = k0 + b;
-        if (k < L) {
-          if (ia < N) wa |= (uint32_t)msa[(long long)ia * L + k] << (8 * b);
-          if (jb < N) wb |= (uint32_t)msa[(long long)jb * L + k] << (8 * b);
-        }
-      }
-      As[r][wd] = wa;
-      Bs[r][wd] = wb;
+    // bytes straight into the word rows (byte b of word wd = column 4 wd + b):
+    // consecutive threads read consecutive bytes of one row, so each warp load
+    // covers one 32-byte sector of the alignment
+    constexpr int kRowBytes = 4 * kRwChunk;
+    for (int e = threadIdx.x; e < kRwTile * kRowBytes; e += blockDim.x) {
+      const int r = e / kRowBytes, bt = e % kRowBytes;
+      const int k = w0 * 4 + bt;
+      const int ia = i0 + r, jb = j0 + r;
+      const bool in = k < L;
+      reinterpret_cast<uint8_t *>(&As[r][0])[bt] =
+          (in && ia < N) ? msa[(long long)ia * L + k] : (uint8_t)0;
+      reinterpret_cast<uint8_t *>(&Bs[r][0])[bt] =
+          (in && jb < N) ? msa[(long long)jb * L + k] : (uint8_t)0;
     }
     __syncthreads();
     const int wmax = (words - w0) < kRwChunk ? (words - w0) : kRwChunk;
@@ -224,17 +222,14 @@ __global__ void __launch_bounds__(256) rw_count_bytes_kernel(const uint8_t *__re
 
 }  // namespace ccm
 
-namespace {
-
-std::mutex g_noalloc_mutex;
-int *g_noalloc_addr[64] = {nullptr};
-
-}  // namespace
-
-// See include/ccmpred_b200.h.  Set-up (first call on a device, under a lock):
-// look up the device address of the count array with cudaGetSymbolAddress
-// while that device is current -- host code must not use the array's name as
-// a device pointer.  After that a call only enqueues a memset and two kernels.
+// See include/ccmpred_b200.h.  Every call looks up the device address of the
+// count array with cudaGetSymbolAddress in the context that is current on the
+// calling thread -- host code must not use the array's name as a device
+// pointer, and an address found in one context (the device's primary context,
+// say) is not valid in another context of the same device.  The lookup
+// allocates nothing once the library's module is loaded in that context (the
+// first call in a context loads it); then a call enqueues a memset and two
+// kernels.
 extern "C" CCM_API int ccm_calculate_weights_noalloc(const unsigned char *d_msa, int ncol,
                                                      int nrow, float threshold, float *d_w,
                                                      void *stream) {
@@ -248,27 +243,15 @@ extern "C" CCM_API int ccm_calculate_weights_noalloc(const unsigned char *d_msa,
                           "sequences",
                           nrow, kNoAllocMaxRows);
   }
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 64) {
-    return set_last_error(CCM_ERR_CUDA, "ccm_calculate_weights_noalloc: no current device (%s)",
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_counts);
+  if (e != cudaSuccess || !p) {
+    return set_last_error(CCM_ERR_CUDA,
+                          "ccm_calculate_weights_noalloc: cudaGetSymbolAddress failed in the "
+                          "current context (%s)",
                           cudaGetErrorString(e));
   }
-  int *counts;
-  {
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev]) {
-      void *p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_noalloc_counts);
-      if (e != cudaSuccess || !p) {
-        return set_last_error(CCM_ERR_CUDA,
-                              "ccm_calculate_weights_noalloc: cudaGetSymbolAddress failed (%s)",
-                              cudaGetErrorString(e));
-      }
-      g_noalloc_addr[dev] = static_cast<int *>(p);
-    }
-    counts = g_noalloc_addr[dev];
-  }
+  int *counts = static_cast<int *>(p);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const float prod = threshold * (float)(uint64_t)ncol;  // src/reweighting.c:10
   const int idthres = (int)ceil((double)prod);

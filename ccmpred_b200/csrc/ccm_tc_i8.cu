@@ -18,6 +18,8 @@
 //
 // One evaluation = colmax (+ the fused CG step), prep (digits of W, g2 <- 2 l2 x,
 // sum x^2), forward, backward, finalize (shared with ccm_tc.cu).
+#include <cmath>
+
 #include <cuda_bf16.h>
 
 #include "ccm_internal.cuh"
@@ -44,6 +46,7 @@ __device__ __forceinline__ bool i8_aborted(const int *abort_flag) {
 
 // 2^s as a float, s in [-126, 127].
 __device__ __forceinline__ float pow2f(int s) { return __int_as_float((s + 127) << 23); }
+inline float pow2_host(int s) { return std::ldexp(1.0f, s); }
 
 // Smallest e with 2^e >= m for the float m with bits `mbits` (m >= 0), limited to
 // [-100, 127] so that 2^(21 - e) stays a normal float; 0 for m == 0.
@@ -444,7 +447,7 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
   double floss = 0.0;
   // R * 2^21 = e * cw - [observed] * won, with cw = w exp(m - M) / S * 2^21
   float cw[kGroupCols];
-  const float won = live ? wn * (float)(1 << kI8FracBits) : 0.0f;
+  const float won = live ? wn * args.r_enc : 0.0f;
 #pragma unroll
   for (int jj = 0; jj < kGroupCols; ++jj) {
     const float mo = other[jj], so = other[kGroupCols + jj];
@@ -485,7 +488,7 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
           const int a = col / kGroupCols, jj = col % kGroupCols;
           t = fmaf(__uint_as_float(v(i)), cw[jj], xr[jj] == a ? -won : 0.0f);
         }
-        // |R| < 1: only the top of the range needs the clamp (P rounding to 1)
+        // |R| 2^-eR <= 1: only the top of the range needs the clamp (P rounding to 1)
         qv[e] = min(__float2int_rn(t), (1 << kI8FracBits) - 1);
       }
       // byte e of each word = digit of element e: d0 = q >> 14, d1 = (q >> 7) & 127,
@@ -520,7 +523,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
   uint64_t *lo_empty = acc_full + 1;
   uint64_t *hi_empty = lo_empty + 1;
   uint64_t *drain = hi_empty + 1;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  // a barrier that no thread ever arrives on: the epilogue waits on it instead
+  // of on acc_full when a test asks for a wait that runs out (acc_wait_cycles)
+  uint64_t *never = drain + 1;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(never + 1);
   int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
   float *tab_scale = reinterpret_cast<float *>(smem + SM::kTabOff);
   float *tab_v = tab_scale + kGroupSlots;
@@ -538,6 +544,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
     mbar_init(lo_empty, 16);
     mbar_init(hi_empty, 16);
     mbar_init(drain, 1);
+    mbar_init(never, 1);
     *abort_flag = 0;
     fence_mbar_init();
   }
@@ -663,6 +670,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
     const int L = args.L;
     const uint32_t lo_bar = mapa_shared(smem_u32(lo_empty), 0);
     const uint32_t hi_bar = mapa_shared(smem_u32(hi_empty), 0);
+
     int local = 0;
     for (int tile = pair; tile < n_tiles; tile += npairs, ++local) {
       // all eight warps finished the previous tile (tables free) and saw no abort
@@ -684,7 +692,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
       }
       named_bar_sync(1, 256);
       const int n = m * kI8PairM + (int)rank * kI8BM + q * 32 + lane;
-      const bool ok = mbar_wait(acc_full, local & 1);
+      // (with acc_wait_cycles set, a wait that runs out by design: see `never`)
+      const bool ok = args.acc_wait_cycles > 0 ? mbar_wait(never, 0, args.acc_wait_cycles)
+                                               : mbar_wait(acc_full, local & 1);
       if (__any_sync(0xffffffffu, !ok)) {
         if (lane == 0) i8_record_error(args.status, kErrFwdTimeout, abort_flag);
         continue;
@@ -810,7 +820,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
   uint64_t *acc_full = empty + kStages;
   uint64_t *acc_empty = acc_full + 1;
   uint64_t *drain = acc_empty + 1;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  // a barrier that no thread ever arrives on: the epilogue waits on it instead
+  // of on acc_full when a test asks for a wait that runs out (acc_wait_cycles)
+  uint64_t *never = drain + 1;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(never + 1);
   int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
   float *tab_scale = reinterpret_cast<float *>(smem + SM::kTabOff);
   float *tab_v = tab_scale + kSpBN;
@@ -827,6 +840,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
     mbar_init(acc_full, 1);
     mbar_init(acc_empty, 16);
     mbar_init(drain, 1);
+    mbar_init(never, 1);
     *abort_flag = 0;
     fence_mbar_init();
   }
@@ -936,6 +950,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
     const int ethr = threadIdx.x - 64;
     const int L = args.L;
     const uint32_t empty_bar = mapa_shared(smem_u32(acc_empty), 0);
+
     int local = 0;
     for (int tile = pair; tile < n_tiles; tile += npairs, ++local) {
       if (named_bar_or(1, 256, i8_aborted(abort_flag))) break;
@@ -955,7 +970,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
       }
       named_bar_sync(1, 256);
       const int n = m * kI8PairM + (int)rank * kI8BM + q * 32 + lane;
-      const bool ok = mbar_wait(acc_full, local & 1);
+      // (with acc_wait_cycles set, a wait that runs out by design: see `never`)
+      const bool ok = args.acc_wait_cycles > 0 ? mbar_wait(never, 0, args.acc_wait_cycles)
+                                               : mbar_wait(acc_full, local & 1);
       if (__any_sync(0xffffffffu, !ok)) {
         if (lane == 0) i8_record_error(args.status, kErrFwdTimeout, abort_flag);
         continue;
@@ -1149,6 +1166,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
     const int L = args.L;
     float *__restrict__ g2 = args.g2;
     float *Tb = reinterpret_cast<float *>(smem + SM::kTOff) + (warp - 2) * 32 * 9;
+    const float r_dec = args.r_dec;
     const uint32_t empty_bar = mapa_shared(smem_u32(acc_empty), 0);
     uint32_t chunk = 0;
     bool ok = true;
@@ -1175,8 +1193,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
             const long long qs = (long long)(int)vh[i] * 16384 + (long long)(int)vl[i];
-            // exact 64-bit sum, one rounding to float, exact scaling by 2^-21
-            accv[c * 16 + i] += __ll2float_rn(qs) * 4.76837158203125e-07f;
+            // exact 64-bit sum, one rounding to float, exact scaling by 2^(eR - 21)
+            accv[c * 16 + i] += __ll2float_rn(qs) * r_dec;
           }
         }
         tc_fence_before();
@@ -1312,6 +1330,8 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   fa.L = L; fa.N = c->N; fa.S = c->S; fa.T = c->T; fa.Npad = c->Npad;
   fa.m_tiles = c->Npad / kI8PairM;
   fa.KP = c->KP;
+  fa.r_enc = pow2_host(kI8FracBits - c->r_exp);
+  fa.acc_wait_cycles = c->acc_wait_cycles;
   const int pair_tiles = fa.m_tiles * c->T;
   const int fpairs = pair_tiles < c->fwd_pairs ? pair_tiles : c->fwd_pairs;
   if (sp)
@@ -1324,6 +1344,7 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   ba.x2 = x2; ba.g2 = g2; ba.g1d = c->d_g1d; ba.tiles = c->d_bwd_tiles;
   ba.n_tiles = c->n_bwd_tiles; ba.status = c->d_status; ba.L = L; ba.S = c->S; ba.Npad = c->Npad;
   ba.lambda_pair = c->lambda_pair;
+  ba.r_dec = pow2_host(c->r_exp - kI8FracBits);
   const int bpairs = c->n_bwd_tiles < c->bwd_pairs ? c->n_bwd_tiles : c->bwd_pairs;
   const bool sym = c->gradient != CCM_GRADIENT_PARTIAL;
   const dim3 bgrid(2 * bpairs);

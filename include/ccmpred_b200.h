@@ -85,6 +85,12 @@ typedef struct ccm_options {
 	                        occupy (rounded down to CTA pairs); 0 = the whole GPU.  Contexts
 	                        that run side by side on one GPU (the batch solver) each take a
 	                        share, so that their persistent kernels stay resident together. */
+	size_t mem_limit;    /* cap on the device memory of this context, in bytes; 0 = none.
+	                        With a cap the context (and the optimizer state of
+	                        ccm_conjugrad_gpu on it) allocates from a private memory pool of
+	                        that maximum size, and an allocation beyond it fails with
+	                        CCM_ERR_NOMEM instead of taking memory that other users of the
+	                        GPU hold. */
 } ccm_options;
 
 /* Result of the last evaluation, as kept on the device. */
@@ -119,8 +125,11 @@ CCM_API long long ccm_nvar_padded(int ncol);
 CCM_API void ccm_options_default(ccm_options *opt, int ncol);
 
 /* Upload the alignment and weights, allocate all device state for `path`.
- * weights == NULL means uniform weights 1.0 (src/reweighting.c:61-67).
- * Replaces init_cuda (src/evaluate_cuda.c:77-139) without process globals. */
+ * weights == NULL means uniform weights 1.0 (src/reweighting.c:61-67); weights
+ * must be finite (any magnitude: the integer paths scale the residuals by a
+ * power of two when a weight exceeds 1).  States above 20 are rejected with
+ * CCM_ERR_INVALID.  Replaces init_cuda (src/evaluate_cuda.c:77-139) without
+ * process globals. */
 CCM_API int ccm_create(ccm_context **ctx, const unsigned char *msa, int ncol, int nrow,
                const float *weights, const ccm_options *opt);
 CCM_API int ccm_destroy(ccm_context *ctx);
@@ -186,6 +195,16 @@ CCM_API long long ccm_launch_count(const ccm_context *ctx);
  * buffer size in bytes; otherwise 0 or a negative status. */
 CCM_API long long ccm_debug_copy(ccm_context *ctx, int which, void *dst, long long bytes);
 
+/* Diagnostics for tests of the bounded waits.  cycles > 0: in the next
+ * evaluations of the integer paths, the forward kernel's epilogue waits, with a
+ * budget of `cycles` SM clock cycles, on a barrier that no thread arrives on
+ * instead of on its accumulator tile.  The wait runs out; the kernel records the
+ * timeout, drains its in-flight copies and MMAs, frees its tensor memory and
+ * returns, and the evaluation reports CCM_ERR_DEVICE.  cycles = 0 restores
+ * normal evaluations; the context stays usable.  No counterpart in the
+ * reference (which has no bounded waits). */
+CCM_API int ccm_debug_set_wait_limit(ccm_context *ctx, long long cycles);
+
 /* Allocation-free sequence reweighting.  No counterpart in the reference.
  *
  * For callers that must not allocate device memory: a process whose memory
@@ -200,8 +219,10 @@ CCM_API long long ccm_debug_copy(ccm_context *ctx, int which, void *dst, long lo
  * routine: its only scratch, one int count per sequence, is a fixed array
  * compiled into the library (1 MiB, nrow <= 262144; larger nrow is rejected
  * with CCM_ERR_INVALID).  Every GPU that loads the library keeps that array
- * until the process exits.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress); after that a call only enqueues a
+ * until the process exits.  Every call looks up the array's device address in
+ * the calling thread's current context (cudaGetSymbolAddress, which allocates
+ * nothing once the library's module is loaded there: the first call in a
+ * context loads it, so make that call before any stream capture) and enqueues a
  * memset and two kernels.  All calls share the array and it keeps the last
  * call's counts (each call clears what it uses first): calls that overlap on
  * the GPU race on it and must be serialised by the caller (one stream, or

@@ -26,6 +26,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libccmoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libccmref.so")
 REF_CUDA_SO = os.path.join(HERE, "_ref", "libccmref_cuda.so")
+# the reference's example alignment (example/1atzA.aln, L=75, N=3068), copied
+# here by oracle/Makefile
+REF_EXAMPLE_ALN = os.path.join(HERE, "_ref", "1atzA.aln")
 
 Q = 21
 QPAD = 32

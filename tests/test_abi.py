@@ -49,7 +49,8 @@ def test_sizes_without_gpu():
 def test_struct_layouts():
     from ccmpred_b200 import _lib
     assert ctypes.sizeof(_lib.CcmResult) == 32
-    assert ctypes.sizeof(_lib.CcmOptions) == 32
+    assert ctypes.sizeof(_lib.CcmOptions) == 40
+    assert _lib.CcmOptions.mem_limit.offset == 32
     # reference userdata: 2 pointers, 4 ints, pointer, 3 floats, pointer (x86-64)
     assert ctypes.sizeof(_lib.CcmUserdata) == 64
     assert _lib.CcmUserdata.extra.offset == 32

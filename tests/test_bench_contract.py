@@ -28,3 +28,6 @@ def test_reference_arm_prints_one_json_line(ref_mod):
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
     assert d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    # the same workload keys as the GPU arm's config, nothing about the implementation
+    assert {"ncol", "nrow", "planted_pairs", "seed", "parallelism"} <= set(d["config"])
+    assert "path" not in d["config"]

@@ -1,0 +1,143 @@
+"""Parity of the tensor-core paths where the product is used, against the FP64
+oracle (a restatement of src/evaluate_cpu.c:16-166) at identical x:
+
+* the headline configuration, L=300, N=5000 (150 planted pairs, reweighting
+  threshold 0.8), at a random admissible x and at x0 = init_bias;
+* an x taken after 5 CG iterations of the device optimizer (the third kind of
+  parity input next to x0 and a random x);
+* a converged, heavy-tailed x: the device CG run to convergence on the
+  reference's example alignment (example/1atzA.aln) -- a few large couplings
+  per column over a background of small ones, the worst case of the integer
+  paths' per-column power-of-two scale;
+* N > 32768 rows at small L, which makes the integer backward cut K into two
+  chunks of at most 32768 rows and merge them;
+* sequence weights above 1 (a library caller's own weighting), which the
+  integer paths encode with a power-of-two residual scale.
+
+Bounds (as in test_gpu_parity): |df|/|f| < 1e-6 and, relative to the L2 norm
+of the whole FP64 gradient, the L2 errors of g, g1 and g2 < 1e-5.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from ccmpred_b200 import Evaluator, calculate_weights, nsingle_padded, synth
+
+pytestmark = pytest.mark.gpu
+
+TC_PATHS = ["tc_i8sp", "tc_i8x3", "tc_bf16x2"]
+TOL = dict(f=1e-6, g=1e-5, g1=1e-5, g2=1e-5)
+
+
+def errors(f, g, f64, g64, L):
+    nsp = nsingle_padded(L)
+    d = g.astype(np.float64) - g64
+    gn = np.linalg.norm(g64)
+    return dict(f=abs(f - f64) / abs(f64), g=float(np.linalg.norm(d) / gn),
+                g1=float(np.linalg.norm(d[:20 * L]) / gn),
+                g2=float(np.linalg.norm(d[nsp:]) / gn))
+
+
+def evaluate(path, msa, w, x, lam1, lam2):
+    import torch
+    with Evaluator(msa, weights=w, lambda_single=lam1, lambda_pair=lam2, path=path) as ev:
+        xd = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float32)).cuda()
+        gd = torch.full_like(xd, float("nan"))
+        f = ev.evaluate(xd, gd)
+        return f, gd.cpu().numpy()
+
+
+def check_paths(oracle_mod, msa, w, x, lam1, lam2, paths=TC_PATHS):
+    L = msa.shape[1]
+    f64, g64 = oracle_mod.oracle_evaluate(msa, w, lam1, lam2, x)
+    for path in paths:
+        f, g = evaluate(path, msa, w, x, lam1, lam2)
+        assert np.all(np.isfinite(g)), path
+        e = errors(f, g, f64, g64, L)
+        assert all(e[k] < TOL[k] for k in TOL), (path, e)
+
+
+@pytest.fixture(scope="module")
+def headline():
+    cfg = synth.PRECISION_300x5000
+    msa = synth.generate(cfg)
+    w = calculate_weights(msa, 0.8)
+    return msa, w
+
+
+@pytest.mark.parametrize("xkind", ["random", "bias"])
+def test_headline_configuration(gpu, oracle_mod, headline, xkind):
+    """L=300, N=5000: the workload the benchmark measures."""
+    from ccmpred_b200.host import init_bias
+    msa, w = headline
+    L = msa.shape[1]
+    x = synth.random_x(L, 1300) if xkind == "random" else init_bias(msa)
+    check_paths(oracle_mod, msa, w, x, 0.01, float(np.float32(0.2) * np.float32(L - 1)))
+
+
+def test_after_five_cg_iterations(gpu, oracle_mod):
+    import torch
+    from ccmpred_b200.host import init_bias
+    msa = synth.generate(synth.SMALL_75x1000)
+    L = msa.shape[1]
+    w = calculate_weights(msa, 0.8)
+    lam2 = float(np.float32(0.2) * np.float32(L - 1))
+    xd = torch.from_numpy(init_bias(msa)).cuda()
+    with Evaluator(msa, weights=w, lambda_pair=lam2) as ev:
+        res = ev.minimize(xd, max_iterations=5, epsilon=0.0)
+    assert res.iterations == 5
+    check_paths(oracle_mod, msa, w, xd.cpu().numpy(), 0.01, lam2,
+                paths=TC_PATHS + ["simt_f32"])
+
+
+def test_converged_heavy_tailed_couplings(gpu, oracle_mod):
+    """The device CG to convergence on the reference's example alignment; the
+    couplings it reaches are heavy-tailed (checked below), the case in which a
+    column's power-of-two scale is set by one large coupling."""
+    import torch
+    from ccmpred_b200.host import init_bias, read_msa
+    if not os.path.exists(oracle_mod.REF_EXAMPLE_ALN):
+        pytest.skip("reference example alignment not copied into oracle/_ref")
+    msa = read_msa(oracle_mod.REF_EXAMPLE_ALN)
+    L = msa.shape[1]
+    w = calculate_weights(msa, 0.8)
+    lam2 = float(np.float32(0.2) * np.float32(L - 1))
+    xd = torch.from_numpy(init_bias(msa)).cuda()
+    with Evaluator(msa, weights=w, lambda_pair=lam2) as ev:
+        res = ev.minimize(xd, max_iterations=250)
+    assert res.iterations > 20
+    x = xd.cpu().numpy()
+    wcoup = np.abs(x[nsingle_padded(L):].reshape(21, L, 32, L)[:, :, :21, :])
+    wcoup = wcoup[wcoup > 0]
+    # heavy tail: the largest couplings are many times the typical one
+    assert wcoup.max() > 5 * np.median(wcoup)
+    check_paths(oracle_mod, msa, w, x, 0.01, lam2)
+
+
+@pytest.mark.parametrize("path", ["tc_i8sp", "tc_i8x3"])
+def test_backward_k_chunks(gpu, oracle_mod, path):
+    """N = 33000 > 32768: the integer backward accumulates two K chunks, each
+    exact in s32, and merges them in FP32."""
+    msa = synth.generate(synth.MSAConfig("kchunk", 24, 33000, n_pairs=4, seed=61))
+    w = calculate_weights(msa, 0.8)
+    x = synth.random_x(24, 62)
+    check_paths(oracle_mod, msa, w, x, 0.01, 0.2 * 23, paths=[path])
+
+
+@pytest.mark.parametrize("path", ["tc_i8sp", "tc_i8x3"])
+@pytest.mark.parametrize("wkind", ["uniform2.5", "spread", "power_of_two"])
+def test_weights_above_one(gpu, oracle_mod, path, wkind):
+    """Residuals w (P - onehot) exceed 1 in magnitude: the integer paths scale
+    them by 2^-ceil(log2 max w) before taking their digits."""
+    msa = synth.generate(synth.MSAConfig("wbig", 40, 600, n_pairs=4, seed=63))
+    N = msa.shape[0]
+    rng = np.random.default_rng(64)
+    if wkind == "uniform2.5":
+        w = np.full(N, 2.5, np.float32)
+    elif wkind == "spread":
+        w = rng.uniform(0.0, 37.0, N).astype(np.float32)
+    else:
+        w = rng.choice(np.array([0.25, 1.0, 4.0], np.float32), N)
+    x = synth.random_x(40, 65)
+    check_paths(oracle_mod, msa, w, x, 0.01, 0.2 * 39, paths=[path])

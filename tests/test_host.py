@@ -47,9 +47,9 @@ def test_output_files_byte_identical(ref_mod, tmp_path):
 
 
 def test_read_msa_matches_reference(ref_mod, tmp_path):
-    path = "/root/reference/example/1atzA.aln"
+    path = ref_mod.REF_EXAMPLE_ALN
     if not os.path.exists(path):
-        pytest.skip("reference example alignment not present")
+        pytest.skip("reference example alignment not copied into oracle/_ref")
     a = host.read_msa(path)
     b = ref_mod.ref_read_msa(path)
     assert a.shape == (3068, 75) and np.array_equal(a, b)

@@ -74,9 +74,9 @@ def test_oracle_weights_bit_exact_vs_reference(ref_mod, thr):
 
 
 def test_oracle_weights_on_example_alignment(ref_mod):
-    path = "/root/reference/example/1atzA.aln"
+    path = ref_mod.REF_EXAMPLE_ALN
     if not os.path.exists(path):
-        pytest.skip("reference example alignment not present")
+        pytest.skip("reference example alignment not copied into oracle/_ref")
     msa = ref_mod.ref_read_msa(path)
     assert msa.shape == (3068, 75)
     a = ref_mod.oracle_weights(msa, 0.8)

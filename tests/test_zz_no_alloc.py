@@ -55,3 +55,31 @@ def test_noalloc_rejects_oversized_input(gpu):
                                              w.data_ptr(), None)
     assert rc == _lib.CCM_ERR_INVALID
     assert b"exceeds the fixed scratch" in lib().ccm_last_error()
+
+
+def test_noalloc_two_streams_ordered_by_an_event(gpu):
+    """Calls on two streams share the scratch; an event that orders the second
+    call after the first (the documented way to serialise them) gives both
+    their exact weights."""
+    import torch
+    a = synth.generate(synth.MSAConfig("na3", 90, 2500, gap_frac=0.2, dup_frac=0.4, seed=43))
+    b = synth.generate(synth.MSAConfig("na4", 47, 1200, gap_frac=0.1, dup_frac=0.6, seed=44))
+    sa, sb = torch.cuda.Stream(), torch.cuda.Stream()
+    outs = []
+    for msa, thr, stream in ((a, 0.8, sa), (b, 0.7, sb)):
+        N, L = msa.shape
+        d_msa = torch.from_numpy(msa).to(gpu)
+        d_w = torch.full((N,), float("nan"), dtype=torch.float32, device=gpu)
+        torch.cuda.synchronize()
+        outs.append((msa, thr, d_msa, d_w))
+    done_a = torch.cuda.Event()
+    msa, thr, d_msa, d_w = outs[0]
+    assert noalloc(d_msa, msa.shape[1], msa.shape[0], thr, d_w, sa.cuda_stream) == _lib.CCM_OK
+    done_a.record(sa)
+    sb.wait_event(done_a)
+    msa, thr, d_msa, d_w = outs[1]
+    assert noalloc(d_msa, msa.shape[1], msa.shape[0], thr, d_w, sb.cuda_stream) == _lib.CCM_OK
+    torch.cuda.synchronize()
+    for msa, thr, _, d_w in outs:
+        expected = calculate_weights(msa, thr)
+        assert np.array_equal(d_w.cpu().numpy().view(np.uint32), expected.view(np.uint32))
