@@ -60,7 +60,8 @@ class CcmCgParams(ctypes.Structure):
     _fields_ = [("max_iterations", ctypes.c_int), ("k", ctypes.c_int),
                 ("max_linesearch", ctypes.c_int), ("pad", ctypes.c_int),
                 ("epsilon", ctypes.c_double), ("alpha_mul", ctypes.c_double),
-                ("ftol", ctypes.c_double), ("wolfe", ctypes.c_double)]
+                ("ftol", ctypes.c_double), ("wolfe", ctypes.c_double),
+                ("min_gnorm", ctypes.c_double)]
 
 
 class CcmCgResult(ctypes.Structure):
@@ -93,12 +94,30 @@ class CcmBatchResult(ctypes.Structure):
                 ("fx", ctypes.c_double), ("seconds", ctypes.c_double)]
 
 
+class ConjugradParams(ctypes.Structure):
+    """conjugrad_parameter_t of include/conjugrad.h (float build)."""
+    _fields_ = [("max_linesearch", ctypes.c_int), ("max_iterations", ctypes.c_int),
+                ("k", ctypes.c_int), ("epsilon", ctypes.c_float), ("ftol", ctypes.c_float),
+                ("wolfe", ctypes.c_float), ("alpha_mul", ctypes.c_float),
+                ("min_gnorm", ctypes.c_float)]
+
+
+CONJUGRAD_SUCCESS = 0
+CONJUGRAD_ALREADY_MINIMIZED = 1
+CONJUGRADERR_UNKNOWN = -1024
+CONJUGRADERR_MAXIMUMITERATION = -1023
+CONJUGRADERR_MAXIMUMLINESEARCH = -1022
+
+# evaluate(instance, x, g, n) -> f  (conjugrad_evaluate_t)
+EVALUATE = ctypes.CFUNCTYPE(ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                            ctypes.c_int)
+
 # progress(instance, x, g, fx, xnorm, gnorm, step, n, k, ls) -> int
 PROGRESS = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                             ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                             ctypes.c_int, ctypes.c_int, ctypes.c_int)
 
-# name -> (restype, argtypes); every symbol include/ccmpred_b200.h declares
+# name -> (restype, argtypes); every symbol include/*.h declares
 _vp = ctypes.c_void_p
 _f32p = ctypes.POINTER(ctypes.c_float)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -162,6 +181,14 @@ SIGNATURES = {
     "evaluate_b200": (ctypes.c_float, [_vp, _f32p, _f32p, ctypes.c_int]),
     "init_b200": (ctypes.c_int, [_vp]),
     "destroy_b200": (ctypes.c_int, [_vp]),
+    # include/conjugrad.h: the optimizer under libconjugrad's names
+    "conjugrad_init": (ctypes.POINTER(ConjugradParams), []),
+    "conjugrad_malloc": (_vp, [ctypes.c_int]),
+    "conjugrad_free": (None, [_vp]),
+    "conjugrad": (ctypes.c_int, [ctypes.c_int, _vp, _f32p, _vp, _vp, _vp,
+                                 ctypes.POINTER(ConjugradParams)]),
+    "conjugrad_gpu": (ctypes.c_int, [ctypes.c_int, _vp, _f32p, _vp, _vp, _vp,
+                                     ctypes.POINTER(ConjugradParams)]),
 }
 
 _lib = None

@@ -25,6 +25,10 @@ void prof_mark(ccm_context *c) {
 
 void count_launch(ccm_context *c, int n) { c->launches += n; }
 
+bool is_context(const void *p) {
+  return p && static_cast<const ccm_context *>(p)->magic == kContextMagic;
+}
+
 cudaError_t dev_alloc_raw(ccm_context *c, void **p, size_t bytes) {
   return c->pool ? cudaMallocFromPoolAsync(p, bytes, c->pool, c->stream)
                  : cudaMallocAsync(p, bytes, c->stream);
@@ -426,9 +430,13 @@ int init_backend(ccm_userdata *ud) {
   if (!ud || !ud->msa || ud->ncol <= 0 || ud->nrow <= 0)
     return set_error(CCM_ERR_INVALID, "init: invalid userdata");
   const int L = ud->ncol, N = ud->nrow;
+  // the device the caller made current (the reference selects it with
+  // cudaSetDevice before init, src/ccmpred.c:421-426)
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
   std::vector<float> w(N, 1.0f);
   if (ud->reweighting_threshold < 1.0f) {
-    int rc = ccm_calculate_weights(ud->msa, L, N, ud->reweighting_threshold, w.data(), 0);
+    int rc = ccm_calculate_weights(ud->msa, L, N, ud->reweighting_threshold, w.data(), dev);
     if (rc != CCM_OK) return rc;
     float wsum = 0.0f, wmin = w[0], wmax = w[0];
     for (int i = 0; i < N; ++i) {
@@ -447,6 +455,7 @@ int init_backend(ccm_userdata *ud) {
   opt.lambda_single = ud->lambda_single;
   opt.lambda_pair = ud->lambda_pair;
   opt.path = g_default_path;
+  opt.device = dev;
   ccm_context *ctx = nullptr;
   int rc = ccm_create(&ctx, ud->msa, L, N, w.data(), &opt);
   if (rc != CCM_OK) return rc;
@@ -632,6 +641,7 @@ int ccm_destroy(ccm_context *ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   free_all(ctx);
+  ctx->magic = 0;
   delete ctx;
   return CCM_OK;
 }

@@ -1,32 +1,31 @@
-// Device-side nonlinear conjugate gradient over the evaluation of a context:
-// the replacement of libconjugrad's conjugrad_gpu (called at src/ccmpred.c:644
-// with the parameters of src/ccmpred.c:526-534; the library itself is absent
-// from the reference checkout, so the rules below are this project's own,
-// written from the parameter names and the standard method, Nocedal & Wright,
-// "Numerical Optimization", 2nd ed., ch. 3 and 5.2):
+// Device-side nonlinear conjugate gradient: the replacement of libconjugrad's
+// conjugrad_gpu (called at src/ccmpred.c:632 with the parameters of
+// src/ccmpred.c:526-534; the library is absent from the reference checkout).
+// The rules -- line search, Polak-Ribiere+ direction, stopping test -- are in
+// ccm_cg_rules.cuh; here they run on the device.
 //
-//   s0 = -g0, alpha0 = 1 / ||g0||
-//   per iteration k:
-//     line search, at most max_linesearch trials x_t = x + alpha s; accept on
-//       sufficient decrease f_t <= f + ftol * alpha * (g.s); otherwise the
-//       next trial is the minimiser of the quadratic through f, g.s and f_t,
-//       safeguarded to [0.1, alpha_mul] times alpha (N&W sec. 3.5);
-//       if all trials fail and s is not -g, restart along s = -g with
-//       alpha = 1/||g|| and search once more
-//     beta = max(0, g_t.(g_t - g) / g.g)                        (Polak-Ribiere+)
-//     s = -g_t + beta s; if s is not a descent direction, s = -g_t
-//     next alpha = 2 (f_old - f_new) / -(g_t.s_new)             (N&W eq. 3.60)
-//     stop when k >= K and (f_{k-K} - f_k) / |f_k| < epsilon    ("-e/-k", src/ccmpred.c:192-196)
-//   The reference's "wolfe" parameter (src/ccmpred.c:533) has no role in these
-//   rules; it is kept in ccm_cg_params for the reference's parameter list.
+// Per line-search trial, on the context's stream:
+//   cg_dir_kernel      s <- -g or -g + beta s when the last decision asks for it
+//   step + evaluation  x_t = x + alpha s (alpha read from the control record;
+//                      fused into the first pass over x on the tensor-core
+//                      paths), f(x_t), g_t
+//   cg_dots_kernel     FP64 partials of g_t.s, g_t.g_t, g_t.g (and x_t.x_t)
+//   cg_control_kernel  one block: the partials summed in a fixed order, then
+//                      one thread applies the rules to the control record and
+//                      sets the conditional nodes' values
+// The trials form the body of a CUDA-graph WHILE node (the line search), and
+// the iterations -- two of them per round, one for each buffer parity, the x
+// and g of one iteration being the trial buffers of the previous one -- the
+// body of an outer WHILE node: without a progress callback the whole solve is
+// one graph launch and the host waits once.  With a progress callback (which
+// the reference calls after every iteration, src/ccmpred.c:50-61) the host
+// launches one line-search graph per iteration and reads the control record
+// back after each.  Vectors stay in float; every dot product and every
+// line-search quantity is FP64.
 //
-// Vectors stay in float on the device; every dot product and the line-search
-// tests are FP64.  One trial step (x_t = x + alpha s, the four evaluation
-// kernels, the dots, the copy of the scalars to pinned host memory) is
-// captured once in a CUDA graph per buffer parity and replayed; the host only
-// reads back 40 bytes per trial.  On the tensor-core paths the step is fused
-// into tc_prep, which reads x and s once and writes x_t while it splits the
-// couplings into their bf16 terms.
+// conjugrad_gpu with another evaluate callback than this library's own
+// (ccm_conjugrad_callback_gpu below) runs the same kernels around one call of
+// the callback per trial, from the host.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -34,6 +33,7 @@
 
 #include <cuda_runtime.h>
 
+#include "ccm_cg_rules.cuh"
 #include "ccm_internal.cuh"
 
 namespace ccm {
@@ -65,8 +65,8 @@ __global__ void cg_step_kernel(const float *__restrict__ x, const float *__restr
     xt[i] = fmaf(a, s[i], x[i]);
 }
 
-// Per-block FP64 partials of  a.b, a.a, a.c  (c may be null).  Fixed grid and
-// fixed summation order: the result does not depend on scheduling.
+// Per-block FP64 partials of  a.b, a.a, a.c  (b and c may be null).  Fixed grid
+// and fixed summation order: the result does not depend on scheduling.
 __global__ void __launch_bounds__(256) cg_dots_kernel(const float *__restrict__ a,
                                                       const float *__restrict__ b,
                                                       const float *__restrict__ c,
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(256) cg_dots_kernel(const float *__restrict__ 
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     const double av = a[i];
-    ab += av * (double)b[i];
+    if (b) ab += av * (double)b[i];
     aa += av * av;
     if (c) ac += av * (double)c[i];
   }
@@ -98,34 +98,85 @@ __global__ void __launch_bounds__(256) cg_dots_kernel(const float *__restrict__ 
   }
 }
 
-// Final FP64 reduction of the dot partials into out[0..2].
-__global__ void cg_dots_final_kernel(const double *__restrict__ part, int nblocks,
-                                     double *__restrict__ out) {
-  __shared__ double red[3][32];
-  double v[3] = {0.0, 0.0, 0.0};
-  for (int i = threadIdx.x; i < nblocks; i += blockDim.x)
-    for (int k = 0; k < 3; ++k) v[k] += part[i * 3 + k];
-  for (int k = 0; k < 3; ++k) {
-    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-    if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = v[k];
-  }
+// s <- -g (dir_mode 1) or fmaf(beta, s, -g) (dir_mode 2); dir_mode 0 keeps s.
+__global__ void cg_dir_kernel(const float *__restrict__ g, float *__restrict__ s,
+                              const CgCtl *__restrict__ ctl, long long n) {
+  const int mode = ctl->dir_mode;
+  if (mode == 0) return;
+  const float b = (float)ctl->beta;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    s[i] = mode == 1 ? -g[i] : fmaf(b, s[i], -g[i]);
+}
+
+// Sum of the partials part[i * 3 + k], i < nblocks, in a fixed order, for a block
+// of 256 threads; the result in thread 0.
+__device__ double reduce_part(const double *part, int nblocks, int k, double *red) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < nblocks; i += blockDim.x) v += part[i * 3 + k];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
   __syncthreads();
-  if (threadIdx.x < 3) {
-    double t = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[threadIdx.x][w];
-    out[threadIdx.x] = t;
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+  __syncthreads();
+  return t;
+}
+
+// Conditional-node values a control kernel sets.  mode 0: none (host-driven);
+// 1: the line search's WHILE only (one graph per iteration); 2: the whole solve
+// (line searches of both parities, the IF that runs the parity-1 iteration, the
+// outer WHILE).
+struct CgHandles {
+  cudaGraphConditionalHandle ls_self, ls_other, it2, outer;
+  int mode, parity;
+};
+
+// After the initial evaluation: f0 (from the evaluation record, or from f_slot
+// when a callback evaluated), g0.g0 from the partials.
+__global__ void __launch_bounds__(256) cg_start_kernel(CgCtl *ctl, const double *part,
+                                                       int nblocks, const ccm_result *res,
+                                                       const double *f_slot) {
+  __shared__ double red[8];
+  const double gg = reduce_part(part, nblocks, 1, red);
+  if (threadIdx.x == 0) {
+    cg_rules_start(*ctl, f_slot ? *f_slot : res->fx, gg);
+    if (res && res->status != 0) {
+      ctl->status = CCM_ERR_DEVICE;
+      ctl->ls_active = 0;
+    }
   }
 }
 
-// s = -g + beta * s  (beta == 0 gives steepest descent).  beta is a launch
-// argument: it is fixed when the kernel is enqueued, with no host buffer that
-// the host could overwrite before the copy runs.
-__global__ void cg_direction_kernel(const float *__restrict__ g, double beta,
-                                    float *__restrict__ s, long long n) {
-  const float b = (float)beta;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    s[i] = fmaf(b, s[i], -g[i]);
+__global__ void __launch_bounds__(256) cg_control_kernel(CgCtl *ctl, CgRuleParams p,
+                                                         const double *part, int nblocks,
+                                                         int with_xx, const ccm_result *res,
+                                                         const double *f_slot, CgHandles h) {
+  __shared__ double red[8];
+  CgTrial t;
+  t.gts = reduce_part(part, nblocks, 0, red);
+  t.gtgt = reduce_part(part, nblocks, 1, red);
+  t.gtg = reduce_part(part, nblocks, 2, red);
+  t.xtxt = with_xx ? reduce_part(part + 3 * nblocks, nblocks, 1, red) : 0.0;
+  if (threadIdx.x != 0) return;
+  t.f = f_slot ? *f_slot : res->fx;
+  t.status = res ? res->status : 0;
+  t.pad = 0;
+  const bool accepted = cg_rules_trial(*ctl, t, p);
+  // a bound on the loop whatever the rules do: two full line searches per iteration
+  if (ctl->status == kCgRunning &&
+      ctl->evals > (p.max_iterations + 1) * 2 * (p.max_linesearch + 1) + 1) {
+    ctl->status = CCM_CG_ERR_LINESEARCH;
+    ctl->ls_active = 0;
+  }
+  const bool running = ctl->status == kCgRunning;
+  if (h.mode >= 1) cudaGraphSetConditional(h.ls_self, ctl->ls_active ? 1u : 0u);
+  if (h.mode == 2 && (accepted || !running)) {
+    cudaGraphSetConditional(h.outer, running ? 1u : 0u);
+    if (h.parity == 0) cudaGraphSetConditional(h.it2, running ? 1u : 0u);
+    cudaGraphSetConditional(h.ls_other, running ? 1u : 0u);
+  }
 }
 
 }  // namespace ccm
@@ -134,101 +185,208 @@ using namespace ccm;
 
 namespace {
 
-// Scalars exchanged with the host per trial (pinned).
-struct TrialOut {
-  double f;      // f(x_t)
-  double gs;     // g_t . s
-  double gg;     // g_t . g_t
-  double ggold;  // g_t . g  (for Polak-Ribiere)
-  double xx;     // x_t . x_t
-  int status;
-  int pad;
-};
-
-struct CgState {
-  ccm_context *c = nullptr;
-  long long n = 0;
-  float *xb[2] = {nullptr, nullptr};  // x ping-pong (xb[0] may be the caller's x)
-  float *gb[2] = {nullptr, nullptr};
-  float *s = nullptr;
-  double *d_alpha = nullptr, *d_part = nullptr, *d_dots = nullptr;
-  double *h_alpha = nullptr;  // pinned
-  TrialOut *h_out = nullptr;  // pinned
-  cudaGraphExec_t trial[2] = {nullptr, nullptr};
-  bool own_x0 = false;
-  bool want_xx = true;   // compute x_t . x_t in every trial (needed by a progress callback)
-  int eval_kernels = 0;  // kernels of the step and the evaluation inside the trial graph
-};
-
-int free_state(CgState &st) {
-  for (int i = 0; i < 2; ++i) {
-    if (st.trial[i]) cudaGraphExecDestroy(st.trial[i]);
-    if ((i == 1 || st.own_x0) && st.xb[i]) cudaFreeAsync(st.xb[i], st.c->stream);
-    if (st.gb[i]) cudaFreeAsync(st.gb[i], st.c->stream);
-  }
-  // stream-ordered frees and pooled pinned slots: nothing here waits for the
-  // other streams of the device
-  for (void *p : {(void *)st.s, (void *)st.d_alpha, (void *)st.d_part, (void *)st.d_dots})
-    if (p) cudaFreeAsync(p, st.c->stream);
-  pinned_small_free(st.h_alpha);
-  pinned_small_free(st.h_out);
-  return CCM_OK;
-}
-
 int grid_for(long long n) {
   const long long b = (n / 4 + 255) / 256;
   return (int)(b < 4 * 148 * 4 ? (b > 0 ? b : 1) : 4 * 148 * 4);
 }
 
-// Enqueue the dots of (a = gt) with (b = s), (a.a), (c = gold) and the copy of
-// f, the dots and x_t.x_t into the pinned TrialOut.
-cudaError_t enqueue_trial_tail(CgState &st, const float *xt, const float *gt, const float *gold) {
-  cudaStream_t s = st.c->stream;
-  cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(gt, st.s, gold, st.n, st.d_part);
-  cg_dots_final_kernel<<<1, 1024, 0, s>>>(st.d_part, kDotBlocks, st.d_dots);
-  if (st.want_xx) {  // ||x_t|| is reported to the progress callback only
-    cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(xt, xt, nullptr, st.n, st.d_part);
-    cg_dots_final_kernel<<<1, 1024, 0, s>>>(st.d_part, kDotBlocks, st.d_dots + 3);
-  }
-  cudaError_t e = cudaMemcpyAsync(&st.h_out->f, &st.c->d_out->fx, sizeof(double),
-                                  cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(&st.h_out->gs, st.d_dots, 3 * sizeof(double), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess && st.want_xx)
-    e = cudaMemcpyAsync(&st.h_out->xx, st.d_dots + 4, sizeof(double), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(&st.h_out->status, &st.c->d_out->status, sizeof(int),
-                        cudaMemcpyDeviceToHost, s);
-  return e;
+CgRuleParams rule_params(const ccm_cg_params &p) {
+  CgRuleParams r;
+  r.max_iterations = p.max_iterations;
+  r.k = p.k;
+  r.max_linesearch = p.max_linesearch;
+  r.pad = 0;
+  r.epsilon = p.epsilon;
+  r.alpha_mul = p.alpha_mul;
+  r.ftol = p.ftol;
+  r.wolfe = p.wolfe;
+  r.min_gnorm = p.min_gnorm;
+  return r;
 }
 
-// Capture: alpha (pinned) -> device; x_t = x + alpha s; evaluate(x_t) -> g_t;
-// dots; scalars -> pinned.  Parity p: x = xb[p], trial into xb[1-p].
-int capture_trial(CgState &st, int p) {
-  cudaStream_t s = st.c->stream;
-  float *x = st.xb[p], *xt = st.xb[1 - p];
-  float *g = st.gb[p], *gt = st.gb[1 - p];
-  cudaGraph_t graph = nullptr;
-  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+int check_params(const ccm_cg_params *p, const char *who) {
+  if (p->max_iterations < 0 || p->k < 1 || p->k >= kCgHist || p->max_linesearch < 1 ||
+      !(p->alpha_mul > 0.0 && p->alpha_mul < 1.0) || !(p->wolfe < 1.0))
+    return set_last_error(CCM_ERR_INVALID, "%s: invalid parameters", who);
+  return CCM_OK;
+}
+
+// Buffers of one solve on a context: x and g of both parities (xb[0] is the
+// caller's x), the direction, the control record and the dot partials.
+struct CgRun {
+  ccm_context *c = nullptr;
+  long long n = 0;
+  float *xb[2] = {nullptr, nullptr};
+  float *gb[2] = {nullptr, nullptr};
+  float *s = nullptr;
+  CgCtl *d_ctl = nullptr;
+  double *d_part = nullptr;
+  CgCtl *h_ctl = nullptr;  // pinned, the kCgCtlHead bytes before fhist
+  cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};  // whole solve | parity 0 | parity 1
+  bool want_xx = false;
+  bool fused = false;
+  int trial_kernels = 0;  // kernels of one trial (launch accounting)
+};
+
+void free_run(CgRun &r) {
+  for (auto &g : r.exec)
+    if (g) cudaGraphExecDestroy(g);
+  cudaStream_t s = r.c->stream;
+  // stream-ordered frees and a pooled pinned slot: nothing here waits for the
+  // other streams of the device
+  for (void *p : {(void *)r.xb[1], (void *)r.gb[0], (void *)r.gb[1], (void *)r.s,
+                  (void *)r.d_ctl, (void *)r.d_part})
+    if (p) cudaFreeAsync(p, s);
+  pinned_small_free(r.h_ctl);
+}
+
+// One trial on the stream (in capture): direction, step + evaluation, dots,
+// control.  Parity p: x = xb[p], trial into xb[1 - p].
+int enqueue_trial(CgRun &r, int p, const CgRuleParams &rp, CgHandles h) {
+  ccm_context *c = r.c;
+  cudaStream_t s = c->stream;
+  float *x = r.xb[p], *xt = r.xb[1 - p], *g = r.gb[p], *gt = r.gb[1 - p];
+  const long long before = c->launches;
+  cg_dir_kernel<<<grid_for(r.n), 256, 0, s>>>(g, r.s, r.d_ctl, r.n);
+  int rc;
+  if (r.fused) {
+    rc = enqueue_evaluation_step(c, x, r.s, &r.d_ctl->alpha, xt, gt);
+  } else {
+    cg_step_kernel<<<grid_for(r.n), 256, 0, s>>>(x, r.s, &r.d_ctl->alpha, xt, r.n);
+    rc = enqueue_evaluation(c, xt, gt);
+  }
+  if (rc != CCM_OK) return rc;
+  cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(gt, r.s, g, r.n, r.d_part);
+  if (r.want_xx) cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(xt, nullptr, nullptr, r.n,
+                                                           r.d_part + 3 * kDotBlocks);
+  cg_control_kernel<<<1, 256, 0, s>>>(r.d_ctl, rp, r.d_part, kDotBlocks, r.want_xx ? 1 : 0,
+                                      c->d_out, nullptr, h);
+  r.trial_kernels = (int)(c->launches - before) + (r.fused ? 0 : 1) + (r.want_xx ? 4 : 3);
+  c->launches = before;  // counted from the evaluations of each run instead
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "cg trial: %s", cudaGetErrorString(e));
+  return CCM_OK;
+}
+
+// Add a conditional node of `type` to `graph` after `deps`; its handle is
+// created on `graph` with `deflt`; the node's body graph is returned.
+cudaError_t add_conditional(cudaGraph_t graph, cudaGraphConditionalNodeType type, unsigned deflt,
+                            const cudaGraphNode_t *deps, size_t ndeps,
+                            cudaGraphConditionalHandle *handle, cudaGraphNode_t *node,
+                            cudaGraph_t *body) {
+  cudaError_t e = cudaGraphConditionalHandleCreate(handle, graph, deflt, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) return e;
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = *handle;
+  np.conditional.type = type;
+  np.conditional.size = 1;
+  e = cudaGraphAddNode(node, graph, deps, ndeps, &np);
+  if (e != cudaSuccess) return e;
+  *body = np.conditional.phGraph_out[0];
+  return cudaSuccess;
+}
+
+// Capture one trial into `body` (the body graph of a WHILE node).
+int capture_trial_into(CgRun &r, cudaGraph_t body, int p, const CgRuleParams &rp, CgHandles h) {
+  cudaStream_t s = r.c->stream;
+  cudaError_t e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "cg capture: %s", cudaGetErrorString(e));
-  cudaMemcpyAsync(st.d_alpha, st.h_alpha, sizeof(double), cudaMemcpyHostToDevice, s);
-  // tensor-core paths take the step inside tc_prep (one pass over x and s that
-  // also splits the couplings into the bf16 terms); the CUDA-core paths step first
-  const bool fused = st.c->path == CCM_PATH_TC_BF16X2 || st.c->path == CCM_PATH_TC_BF16X3 ||
-                     st.c->path == CCM_PATH_TC_I8X3 || st.c->path == CCM_PATH_TC_I8SP;
-  if (!fused) cg_step_kernel<<<grid_for(st.n), 256, 0, s>>>(x, st.s, st.d_alpha, xt, st.n);
-  const long long before = st.c->launches;
-  int rc = fused ? enqueue_evaluation_step(st.c, x, st.s, st.d_alpha, xt, gt)
-                 : enqueue_evaluation(st.c, xt, gt);
-  st.eval_kernels = (int)(st.c->launches - before) + (fused ? 0 : 1);
-  st.c->launches = before;  // counted per replay instead
-  e = enqueue_trial_tail(st, xt, gt, g);
-  cudaError_t e2 = cudaStreamEndCapture(s, &graph);
-  if (rc != CCM_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
+  const int rc = enqueue_trial(r, p, rp, h);
+  cudaGraph_t out = nullptr;
+  e = cudaStreamEndCapture(s, &out);
+  if (rc != CCM_OK) return rc;
+  if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "cg capture: %s", cudaGetErrorString(e));
+  return CCM_OK;
+}
+
+// The copy of the control record's scalars to pinned memory, appended to
+// `graph` after `dep`.
+int capture_readback(CgRun &r, cudaGraph_t graph, cudaGraphNode_t dep) {
+  cudaStream_t s = r.c->stream;
+  cudaError_t e = cudaStreamBeginCaptureToGraph(s, graph, &dep, nullptr, 1,
+                                                cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(r.h_ctl, r.d_ctl, kCgCtlHead, cudaMemcpyDeviceToHost, s);
+  cudaGraph_t out = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(s, &out);
   if (e == cudaSuccess) e = e2;
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&st.trial[p], graph, 0);
-  if (graph) cudaGraphDestroy(graph);
   if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "cg capture: %s", cudaGetErrorString(e));
+  return CCM_OK;
+}
+
+// Whole solve: WHILE(outer) { WHILE(ls0) { trial parity 0 }; IF(it2) { WHILE(ls1)
+// { trial parity 1 } } }, then the read-back.
+int build_solve_graph(CgRun &r, const CgRuleParams &rp) {
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaGraphCreate(&g, 0);
+  if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "cg graph: %s", cudaGetErrorString(e));
+  cudaGraphConditionalHandle h_out, h_ls0, h_it2, h_ls1;
+  cudaGraphNode_t n_out, n_ls0, n_it2, n_ls1;
+  cudaGraph_t b_out, b_ls0, b_it2, b_ls1;
+  e = add_conditional(g, cudaGraphCondTypeWhile, 1, nullptr, 0, &h_out, &n_out, &b_out);
+  if (e == cudaSuccess)
+    e = add_conditional(b_out, cudaGraphCondTypeWhile, 1, nullptr, 0, &h_ls0, &n_ls0, &b_ls0);
+  if (e == cudaSuccess)
+    e = add_conditional(b_out, cudaGraphCondTypeIf, 0, &n_ls0, 1, &h_it2, &n_it2, &b_it2);
+  if (e == cudaSuccess)
+    e = add_conditional(b_it2, cudaGraphCondTypeWhile, 1, nullptr, 0, &h_ls1, &n_ls1, &b_ls1);
+  int rc = CCM_OK;
+  if (e != cudaSuccess) rc = set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
+  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls0, 0, rp, CgHandles{h_ls0, h_ls1, h_it2, h_out, 2, 0});
+  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls1, 1, rp, CgHandles{h_ls1, h_ls0, h_it2, h_out, 2, 1});
+  if (rc == CCM_OK) rc = capture_readback(r, g, n_out);
+  if (rc == CCM_OK) {
+    e = cudaGraphInstantiate(&r.exec[0], g, 0);
+    if (e != cudaSuccess) rc = set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
+  }
+  cudaGraphDestroy(g);
+  return rc;
+}
+
+// One iteration of parity p: WHILE(ls) { trial }, then the read-back.
+int build_iteration_graph(CgRun &r, int p, const CgRuleParams &rp) {
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaGraphCreate(&g, 0);
+  if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "cg graph: %s", cudaGetErrorString(e));
+  cudaGraphConditionalHandle h_ls;
+  cudaGraphNode_t n_ls;
+  cudaGraph_t b_ls;
+  e = add_conditional(g, cudaGraphCondTypeWhile, 1, nullptr, 0, &h_ls, &n_ls, &b_ls);
+  int rc = e == cudaSuccess ? CCM_OK
+                            : set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
+  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls, p, rp, CgHandles{h_ls, h_ls, h_ls, h_ls, 1, p});
+  if (rc == CCM_OK) rc = capture_readback(r, g, n_ls);
+  if (rc == CCM_OK) {
+    e = cudaGraphInstantiate(&r.exec[1 + p], g, 0);
+    if (e != cudaSuccess) rc = set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
+  }
+  cudaGraphDestroy(g);
+  return rc;
+}
+
+int finish(CgRun &r, float *d_x, ccm_cg_result *result, int stopped) {
+  ccm_context *c = r.c;
+  const CgCtl &h = *r.h_ctl;
+  cudaError_t e = cudaSuccess;
+  // leave the final x in the caller's buffer
+  if (h.parity == 1)
+    e = cudaMemcpyAsync(d_x, r.xb[1], sizeof(float) * (size_t)r.n, cudaMemcpyDeviceToDevice,
+                        c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  ccm_cg_result res;
+  std::memset(&res, 0, sizeof(res));
+  res.status = stopped ? CCM_CG_STOPPED : h.status;
+  res.iterations = h.iter;
+  res.evaluations = h.evals;
+  res.fx = h.f;
+  res.gnorm = std::sqrt(h.gg);
+  const int dev_err = h.status == CCM_ERR_DEVICE;
+  free_run(r);
+  if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "ccm_conjugrad_gpu: %s", cudaGetErrorString(e));
+  if (dev_err) return set_last_error(CCM_ERR_DEVICE, "ccm_conjugrad_gpu: device wait timed out in an evaluation");
+  if (result) *result = res;
   return CCM_OK;
 }
 
@@ -238,14 +396,15 @@ extern "C" {
 
 void ccm_cg_params_default(ccm_cg_params *p) {
   if (!p) return;
-  // src/ccmpred.c:222-229, 526-534
+  // src/ccmpred.c:222-229, 526-534, as the reference holds them (float)
   p->max_iterations = 250;
-  p->epsilon = 0.01;
+  p->epsilon = (double)0.01f;
   p->k = 5;
   p->max_linesearch = 5;
   p->alpha_mul = 0.5;
-  p->ftol = 1e-4;
-  p->wolfe = 0.2;
+  p->ftol = (double)1e-4f;
+  p->wolfe = (double)0.2f;
+  p->min_gnorm = 0.0;
 }
 
 int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_params *params,
@@ -255,165 +414,253 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
     return set_last_error(CCM_ERR_INVALID, "ccm_conjugrad_gpu: n %lld != nvar_padded %lld", n, c->nvarp);
   if (c->path == CCM_PATH_SIMT_F64)
     return set_last_error(CCM_ERR_INVALID, "ccm_conjugrad_gpu: needs a float evaluation path");
-  if (params->max_iterations < 0 || params->k < 1 || params->max_linesearch < 1 ||
-      !(params->alpha_mul > 0.0 && params->alpha_mul < 1.0))
-    return set_last_error(CCM_ERR_INVALID, "ccm_conjugrad_gpu: invalid parameters");
+  int rc = check_params(params, "ccm_conjugrad_gpu");
+  if (rc != CCM_OK) return rc;
   cudaSetDevice(c->device);
   cudaStream_t s = c->stream;
-  CgState st;
-  st.c = c;
-  st.n = n;
-  st.xb[0] = d_x;
-  st.want_xx = progress != nullptr;
+  const CgRuleParams rp = rule_params(*params);
+  CgRun r;
+  r.c = c;
+  r.n = n;
+  r.xb[0] = d_x;
+  r.want_xx = progress != nullptr;
+  // tensor-core paths take the step inside the first pass over x
+  r.fused = c->path == CCM_PATH_TC_BF16X2 || c->path == CCM_PATH_TC_BF16X3 ||
+            c->path == CCM_PATH_TC_I8X3 || c->path == CCM_PATH_TC_I8SP;
   const size_t bytes = sizeof(float) * (size_t)n;
   cudaError_t e = cudaSuccess;
-  auto chk = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
-  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&st.xb[1]), bytes));
-  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&st.gb[0]), bytes));
-  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&st.gb[1]), bytes));
-  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&st.s), bytes));
-  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&st.d_alpha), sizeof(double)));
-  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&st.d_part), sizeof(double) * 3 * kDotBlocks));
-  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&st.d_dots), sizeof(double) * 6));
-  static_assert(sizeof(TrialOut) <= 256, "TrialOut must fit a pinned slot");
-  st.h_alpha = static_cast<double *>(pinned_small_alloc(sizeof(double)));
-  st.h_out = static_cast<TrialOut *>(pinned_small_alloc(sizeof(TrialOut)));
-  if (!st.h_alpha || !st.h_out) chk(cudaErrorMemoryAllocation);
+  auto chk = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&r.xb[1]), bytes));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&r.gb[0]), bytes));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&r.gb[1]), bytes));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&r.s), bytes));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&r.d_ctl), sizeof(CgCtl)));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&r.d_part), sizeof(double) * 6 * kDotBlocks));
+  static_assert(kCgCtlHead <= 256, "the control record's scalars must fit a pinned slot");
+  r.h_ctl = static_cast<CgCtl *>(pinned_small_alloc(kCgCtlHead));
+  if (!r.h_ctl) chk(cudaErrorMemoryAllocation);
   if (e != cudaSuccess) {
-    free_state(st);
+    free_run(r);
     (void)cudaGetLastError();  // a failed allocation must not surface in a later launch check
     return set_last_error(e == cudaErrorMemoryAllocation ? CCM_ERR_NOMEM : CCM_ERR_CUDA,
                           "ccm_conjugrad_gpu: %s", cudaGetErrorString(e));
   }
-  ccm_cg_result res;
-  std::memset(&res, 0, sizeof(res));
-  int p = 0;  // x = xb[p], g = gb[p]
+  // profiling marks are not captured into the solve's graphs
+  const bool prof = c->prof_on;
+  c->prof_on = false;
 
-  // initial evaluation: f0, g0 and the dots with s := 0 (g.s unused)
-  cudaMemsetAsync(st.s, 0, bytes, s);
-  int rc = enqueue_evaluation(c, st.xb[0], st.gb[0]);
+  // initial evaluation at x0: f0, g0, g0.g0
+  rc = enqueue_evaluation(c, r.xb[0], r.gb[0]);
   if (rc == CCM_OK) {
-    e = enqueue_trial_tail(st, st.xb[0], st.gb[0], st.gb[0]);
+    cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(r.gb[0], nullptr, nullptr, n, r.d_part);
+    cg_start_kernel<<<1, 256, 0, s>>>(r.d_ctl, r.d_part, kDotBlocks, c->d_out, nullptr);
+    count_launch(c, 2);
+    e = cudaMemcpyAsync(r.h_ctl, r.d_ctl, kCgCtlHead, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) rc = set_last_error(CCM_ERR_CUDA, "ccm_conjugrad_gpu: %s", cudaGetErrorString(e));
   }
-  if (rc == CCM_OK && st.h_out->status != 0)
-    rc = set_last_error(CCM_ERR_DEVICE, "ccm_conjugrad_gpu: device wait timed out in evaluation");
-  if (rc != CCM_OK) { free_state(st); return rc; }
-  double f = st.h_out->f, gg = st.h_out->gg;
-  res.evaluations = 1;
-  std::vector<double> fhist;
-  fhist.push_back(f);
-  if (!(gg > 0.0) || !std::isfinite(f)) {
-    res.status = std::isfinite(f) ? CCM_CG_ALREADY_MINIMIZED : CCM_CG_ERR_NONFINITE;
-    res.fx = f;
-    free_state(st);
-    if (result) *result = res;
-    return CCM_OK;
+  // the graphs: the whole solve without a progress callback, else one per parity
+  if (rc == CCM_OK && r.h_ctl->status == kCgRunning) {
+    if (!progress) {
+      rc = build_solve_graph(r, rp);
+    } else {
+      rc = build_iteration_graph(r, 0, rp);
+      if (rc == CCM_OK) rc = build_iteration_graph(r, 1, rp);
+    }
   }
-  // s0 = -g0
-  cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[0], 0.0, st.s, n);
-  double gs = -gg;  // g.s with s = -g
-  double alpha = 1.0 / std::sqrt(gg);
-  bool steepest = true;  // s == -g
-  int status = CCM_CG_ERR_MAXITER;
-  for (int k = 1; k <= params->max_iterations; ++k) {
-    bool accepted = false;
-    int ls = 0, trials = 0;
-    for (int attempt = 0; attempt < 2 && !accepted; ++attempt) {
-      for (ls = 1; ls <= params->max_linesearch; ++ls) {
-        if (!st.trial[p]) {
-          rc = capture_trial(st, p);
-          if (rc != CCM_OK) { free_state(st); return rc; }
-        }
-        *st.h_alpha = alpha;
-        e = cudaGraphLaunch(st.trial[p], s);
-        // (step +) evaluation + (1 or 2) x (dots + final)
-        c->launches += st.eval_kernels + (st.want_xx ? 4 : 2);
+  c->prof_on = prof;
+  if (rc != CCM_OK) { free_run(r); return rc; }
+
+  int stopped = 0;
+  if (r.h_ctl->status == kCgRunning) {
+    if (!progress) {
+      e = cudaGraphLaunch(r.exec[0], s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    } else {
+      while (e == cudaSuccess && r.h_ctl->status == kCgRunning) {
+        const int iter0 = r.h_ctl->iter;
+        e = cudaGraphLaunch(r.exec[1 + r.h_ctl->parity], s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) {
-          free_state(st);
-          return set_last_error(CCM_ERR_CUDA, "ccm_conjugrad_gpu: %s", cudaGetErrorString(e));
-        }
-        res.evaluations++;
-        trials++;
-        if (st.h_out->status != 0) {
-          free_state(st);
-          return set_last_error(CCM_ERR_DEVICE, "ccm_conjugrad_gpu: device wait timed out in evaluation");
-        }
-        const double ft = st.h_out->f;
-        if (std::isfinite(ft) && ft <= f + params->ftol * alpha * gs) {
-          accepted = true;
+        if (e != cudaSuccess) break;
+        const CgCtl &h = *r.h_ctl;
+        if (h.iter > iter0 &&
+            progress(instance, r.xb[h.parity], r.gb[h.parity], (float)h.f, (float)std::sqrt(h.xx),
+                     (float)std::sqrt(h.gg), (float)h.step, (int)n, h.iter, h.ls_last)) {
+          stopped = 1;
           break;
         }
-        const double den = 2.0 * (ft - f - gs * alpha);
-        double aq = (std::isfinite(ft) && den > 0.0) ? -gs * alpha * alpha / den
-                                                    : params->alpha_mul * alpha;
-        aq = std::fmin(aq, params->alpha_mul * alpha);
-        alpha = std::fmax(aq, 0.1 * alpha);
-      }
-      if (!accepted && !steepest) {
-        // restart along the steepest-descent direction
-        cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[p], 0.0, st.s, n);
-        c->launches += 1;
-        gs = -gg;
-        alpha = 1.0 / std::sqrt(gg);
-        steepest = true;
-      } else if (!accepted) {
-        break;
       }
     }
-    if (!accepted) { status = CCM_CG_ERR_LINESEARCH; break; }
-    ls = trials;
-    // accept: x, g <- trial buffers
-    const double fnew = st.h_out->f, ggnew = st.h_out->gg, gtg = st.h_out->ggold;
-    const double xx = st.h_out->xx;
-    p = 1 - p;
-    const double step = alpha;
-    // Polak-Ribiere+ direction
-    double beta = (ggnew - gtg) / gg;
-    if (!(beta > 0.0)) beta = 0.0;
-    steepest = beta == 0.0;
-    cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[p], beta, st.s, n);
-    c->launches += 1;
-    // g.s for the new direction: -||g||^2 + beta * (g_t.s_old)
-    double gs_new = -ggnew + beta * st.h_out->gs;
-    if (!(gs_new < 0.0)) {
-      // not a descent direction: restart with steepest descent
-      cg_direction_kernel<<<grid_for(n), 256, 0, s>>>(st.gb[p], 0.0, st.s, n);
-      gs_new = -ggnew;
-      steepest = true;
-    }
-    alpha = 2.0 * (f - fnew) / -gs_new;
-    gs = gs_new;
-    f = fnew;
-    gg = ggnew;
-    fhist.push_back(f);
-    res.iterations = k;
-    if (progress) {
-      e = cudaStreamSynchronize(s);
-      const int stop = progress(instance, st.xb[p], st.gb[p], (float)f, (float)std::sqrt(xx),
-                                (float)std::sqrt(gg), (float)step, (int)n, k, ls);
-      if (stop) { status = CCM_CG_STOPPED; break; }
-    }
-    if (k >= params->k) {
-      const double fk = fhist[fhist.size() - 1 - params->k];
-      if ((fk - f) / std::fabs(f) < params->epsilon) { status = CCM_CG_SUCCESS; break; }
+    if (e != cudaSuccess) {
+      free_run(r);
+      return set_last_error(CCM_ERR_CUDA, "ccm_conjugrad_gpu: %s", cudaGetErrorString(e));
     }
   }
-  // leave the final x in the caller's buffer
-  if (p == 1) cudaMemcpyAsync(d_x, st.xb[1], bytes, cudaMemcpyDeviceToDevice, s);
-  e = cudaStreamSynchronize(s);
-  res.fx = f;
-  res.gnorm = std::sqrt(gg);
-  res.status = status;
-  free_state(st);
-  if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "ccm_conjugrad_gpu: %s", cudaGetErrorString(e));
+  c->launches += (long long)(r.h_ctl->evals - 1) * r.trial_kernels;
+  return finish(r, d_x, result, stopped);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- callback CG
+// conjugrad_gpu with an evaluate callback that is not this library's own: the
+// same kernels and rules, one host call of the callback per trial, on the legacy
+// default stream (the stream of the reference's evaluate_cuda).
+int ccm::conjugrad_callback_gpu(float *d_x, long long n, ccm_eval_callback eval,
+                                ccm_progress_t progress, void *instance,
+                                const ccm_cg_params *params, ccm_cg_result *result) {
+  int rc = check_params(params, "conjugrad_gpu");
+  if (rc != CCM_OK) return rc;
+  const CgRuleParams rp = rule_params(*params);
+  cudaStream_t s = 0;  // legacy default stream
+  const size_t bytes = sizeof(float) * (size_t)n;
+  float *xb[2] = {d_x, nullptr}, *gb[2] = {nullptr, nullptr}, *dir = nullptr;
+  CgCtl *d_ctl = nullptr;
+  double *d_part = nullptr, *d_f = nullptr;
+  cudaError_t e = cudaMallocAsync(&xb[1], bytes, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&gb[0], bytes, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&gb[1], bytes, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&dir, bytes, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_ctl, sizeof(CgCtl), s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_part, sizeof(double) * 6 * kDotBlocks, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_f, sizeof(double), s);
+  CgCtl *h = static_cast<CgCtl *>(pinned_small_alloc(kCgCtlHead));
+  double *h_f = static_cast<double *>(pinned_small_alloc(sizeof(double)));
+  if (e == cudaSuccess && (!h || !h_f)) e = cudaErrorMemoryAllocation;
+  const CgHandles none{0, 0, 0, 0, 0, 0};
+  int stopped = 0;
+  // one evaluation by the callback at xb[q] into gb[q]; its f goes to the device
+  auto evaluate = [&](int q) -> cudaError_t {
+    cudaError_t r = cudaStreamSynchronize(s);  // x complete before the callback reads it
+    if (r != cudaSuccess) return r;
+    *h_f = (double)eval(instance, xb[q], gb[q], (int)n);
+    return cudaMemcpyAsync(d_f, h_f, sizeof(double), cudaMemcpyHostToDevice, s);
+  };
+  if (e == cudaSuccess) e = evaluate(0);
+  if (e == cudaSuccess) {
+    cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(gb[0], nullptr, nullptr, n, d_part);
+    cg_start_kernel<<<1, 256, 0, s>>>(d_ctl, d_part, kDotBlocks, nullptr, d_f);
+    e = cudaMemcpyAsync(h, d_ctl, kCgCtlHead, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  }
+  while (e == cudaSuccess && h->status == kCgRunning) {
+    const int p = h->parity, iter0 = h->iter;
+    cg_dir_kernel<<<grid_for(n), 256, 0, s>>>(gb[p], dir, d_ctl, n);
+    cg_step_kernel<<<grid_for(n), 256, 0, s>>>(xb[p], dir, &d_ctl->alpha, xb[1 - p], n);
+    e = evaluate(1 - p);
+    if (e != cudaSuccess) break;
+    cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(gb[1 - p], dir, gb[p], n, d_part);
+    if (progress) cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(xb[1 - p], nullptr, nullptr, n,
+                                                           d_part + 3 * kDotBlocks);
+    cg_control_kernel<<<1, 256, 0, s>>>(d_ctl, rp, d_part, kDotBlocks, progress ? 1 : 0, nullptr,
+                                        d_f, none);
+    e = cudaMemcpyAsync(h, d_ctl, kCgCtlHead, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && progress && h->iter > iter0 &&
+        progress(instance, xb[h->parity], gb[h->parity], (float)h->f, (float)std::sqrt(h->xx),
+                 (float)std::sqrt(h->gg), (float)h->step, (int)n, h->iter, h->ls_last)) {
+      stopped = 1;
+      break;
+    }
+  }
+  ccm_cg_result res;
+  std::memset(&res, 0, sizeof(res));
+  if (e == cudaSuccess && h->parity == 1)
+    e = cudaMemcpyAsync(d_x, xb[1], bytes, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) {
+    res.status = stopped ? CCM_CG_STOPPED : h->status;
+    res.iterations = h->iter;
+    res.evaluations = h->evals;
+    res.fx = h->f;
+    res.gnorm = std::sqrt(h->gg);
+  }
+  for (void *p : {(void *)xb[1], (void *)gb[0], (void *)gb[1], (void *)dir, (void *)d_ctl,
+                  (void *)d_part, (void *)d_f})
+    if (p) cudaFreeAsync(p, s);
+  pinned_small_free(h);
+  pinned_small_free(h_f);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return set_last_error(e == cudaErrorMemoryAllocation ? CCM_ERR_NOMEM : CCM_ERR_CUDA,
+                          "conjugrad_gpu: %s", cudaGetErrorString(e));
+  }
   if (result) *result = res;
   return CCM_OK;
 }
 
-}  // extern "C"
+// ---------------------------------------------------------------- host-vector CG
+// conjugrad: host x, a callback with host pointers.  The same rules
+// (ccm_cg_rules.cuh) on the host; dot products accumulate in FP64 in a fixed
+// order, the vector updates are the device kernels' float operations.
+int ccm::conjugrad_host_vectors(float *x, long long n, ccm_eval_callback eval,
+                                ccm_progress_t progress, void *instance,
+                                const ccm_cg_params *params, ccm_cg_result *result) {
+  int rc = check_params(params, "conjugrad");
+  if (rc != CCM_OK) return rc;
+  const CgRuleParams rp = rule_params(*params);
+  std::vector<float> xo((size_t)n), g0((size_t)n), g1((size_t)n), dir((size_t)n);
+  float *xb[2] = {x, xo.data()}, *gb[2] = {g0.data(), g1.data()};
+  std::vector<double> fhist;
+  CgCtl c;
+  std::memset(&c, 0, sizeof(c));
+  auto dots = [&](const float *a, const float *b, const float *d, double out[3]) {
+    double ab = 0.0, aa = 0.0, ad = 0.0;
+    for (long long i = 0; i < n; ++i) {
+      const double av = a[i];
+      if (b) ab += av * (double)b[i];
+      aa += av * av;
+      if (d) ad += av * (double)d[i];
+    }
+    out[0] = ab;
+    out[1] = aa;
+    out[2] = ad;
+  };
+  double d3[3];
+  const double f0 = (double)eval(instance, xb[0], gb[0], (int)n);
+  dots(gb[0], nullptr, nullptr, d3);
+  cg_rules_start(c, f0, d3[1]);
+  int stopped = 0;
+  while (c.status == kCgRunning) {
+    const int p = c.parity, iter0 = c.iter;
+    float *xp = xb[p], *xt = xb[1 - p], *gp = gb[p], *gt = gb[1 - p];
+    if (c.dir_mode != 0) {
+      const float b = (float)c.beta;
+      for (long long i = 0; i < n; ++i)
+        dir[(size_t)i] = c.dir_mode == 1 ? -gp[i] : fmaf(b, dir[(size_t)i], -gp[i]);
+    }
+    const float a = (float)c.alpha;
+    for (long long i = 0; i < n; ++i) xt[i] = fmaf(a, dir[(size_t)i], xp[i]);
+    CgTrial t;
+    std::memset(&t, 0, sizeof(t));
+    t.f = (double)eval(instance, xt, gt, (int)n);
+    dots(gt, dir.data(), gp, d3);
+    t.gts = d3[0];
+    t.gtgt = d3[1];
+    t.gtg = d3[2];
+    if (progress) {
+      dots(xt, nullptr, nullptr, d3);
+      t.xtxt = d3[1];
+    }
+    cg_rules_trial(c, t, rp);
+    if (progress && c.iter > iter0 &&
+        progress(instance, xb[c.parity], gb[c.parity], (float)c.f, (float)std::sqrt(c.xx),
+                 (float)std::sqrt(c.gg), (float)c.step, (int)n, c.iter, c.ls_last)) {
+      stopped = 1;
+      break;
+    }
+  }
+  if (c.parity == 1) std::memcpy(x, xb[1], sizeof(float) * (size_t)n);
+  if (result) {
+    std::memset(result, 0, sizeof(*result));
+    result->status = stopped ? CCM_CG_STOPPED : c.status;
+    result->iterations = c.iter;
+    result->evaluations = c.evals;
+    result->fx = c.f;
+    result->gnorm = std::sqrt(c.gg);
+  }
+  return CCM_OK;
+}
 
 extern "C" int ccm_conjugrad_host(ccm_context *c, float *x, long long n, const ccm_cg_params *params,
                                   ccm_progress_t progress, void *instance, ccm_cg_result *result) {
@@ -424,8 +671,10 @@ extern "C" int ccm_conjugrad_host(ccm_context *c, float *x, long long n, const c
   float *d_x = nullptr;
   const size_t bytes = sizeof(float) * (size_t)n;
   cudaError_t e = dev_alloc_raw(c, reinterpret_cast<void **>(&d_x), bytes);
-  if (e != cudaSuccess)
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
     return set_last_error(CCM_ERR_NOMEM, "ccm_conjugrad_host: %s", cudaGetErrorString(e));
+  }
   e = cudaMemcpyAsync(d_x, x, bytes, cudaMemcpyHostToDevice, c->stream);
   int rc = CCM_OK;
   if (e == cudaSuccess) rc = ccm_conjugrad_gpu(c, d_x, n, params, progress, instance, result);

@@ -181,9 +181,25 @@ int enqueue_evaluation_step(ccm_context *c, const float *d_x, const float *d_s,
 cudaError_t reweight_counts(const uint8_t *d_msa, int L, int N, int idthres, int *d_counts,
                             cudaStream_t stream);
 
+// An evaluate callback of the reference's shape (include/evaluate_cuda.h:8-13).
+typedef float (*ccm_eval_callback)(void *instance, const float *x, float *g, const int n);
+// The device CG around a foreign callback (device x; one callback call per trial).
+int conjugrad_callback_gpu(float *d_x, long long n, ccm_eval_callback eval,
+                           ccm_progress_t progress, void *instance, const ccm_cg_params *params,
+                           ccm_cg_result *result);
+// The same rules over host vectors (host x; the callback gets host pointers).
+int conjugrad_host_vectors(float *x, long long n, ccm_eval_callback eval,
+                           ccm_progress_t progress, void *instance, const ccm_cg_params *params,
+                           ccm_cg_result *result);
+// True when p points at a live context of this library.
+bool is_context(const void *p);
+
+constexpr uint32_t kContextMagic = 0xCC3B2000u;
+
 }  // namespace ccm
 
 struct ccm_context {
+  uint32_t magic = ccm::kContextMagic;  // cleared when the context is destroyed
   int device = 0;
   int num_sms = 148;
   int fwd_pairs = 74;             // resident CTA pairs of tc_forward

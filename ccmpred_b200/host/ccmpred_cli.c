@@ -64,7 +64,9 @@ int main(int argc, char **argv) {
 	char *rawfilename = NULL, *initfilename = NULL;
 	int numiter = 250, use_apc = 1, use_normalization = 0, conjugrad_k = 5, device = 0;
 	float lambda_single = 0.01f, lambda_pair_factor = 0.2f, reweighting_threshold = 0.8f;
-	double conjugrad_eps = 0.01;
+	/* float, as the reference holds it (src/ccmpred.c:229,312,529): the stopping test
+	 * then uses the same threshold as the reference's own driver does */
+	float conjugrad_eps = 0.01f;
 	int opt;
 	while ((opt = getopt(argc, argv, "r:i:n:w:k:e:l:d:t:ARh?")) != -1) {
 		switch (opt) {
@@ -74,7 +76,7 @@ int main(int argc, char **argv) {
 			case 'w': reweighting_threshold = (float)atof(optarg); break;
 			case 'l': lambda_pair_factor = (float)atof(optarg); break;
 			case 'k': conjugrad_k = atoi(optarg); break;
-			case 'e': conjugrad_eps = atof(optarg); break;
+			case 'e': conjugrad_eps = (float)atof(optarg); break;
 			case 'd': device = atoi(optarg); break;
 			case 't': break;
 			case 'A': use_apc = 0; break;

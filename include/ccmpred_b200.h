@@ -239,8 +239,13 @@ CCM_API void ccm_set_default_path(int path);
 /* ---------------------------------------------------------------- optimizer */
 /* Device-side nonlinear conjugate gradient over a context's evaluation; the
  * replacement of libconjugrad's conjugrad_gpu (src/ccmpred.c:632-648, absent
- * from the reference checkout).  Parameters as set at src/ccmpred.c:526-534;
- * FP64 line-search tests and dot products, float vectors on the device. */
+ * from the reference checkout; the libconjugrad names themselves are in
+ * conjugrad.h).  Parameters as set at src/ccmpred.c:526-534 (the defaults are
+ * the reference's float values); FP64 line-search tests and dot products,
+ * float vectors on the device.  The line search, the direction update and the
+ * stopping test run on the device: without a progress callback the whole solve
+ * is one CUDA-graph launch (conditional WHILE/IF nodes), with one the host
+ * waits once per iteration to call it. */
 typedef struct ccm_cg_params {
 	int max_iterations;   /* -n, default 250 (src/ccmpred.c:222) */
 	int k;                /* -k, default 5: convergence window */
@@ -249,7 +254,9 @@ typedef struct ccm_cg_params {
 	double epsilon;       /* -e, default 0.01: stop when (f_{i-k} - f_i)/|f_i| < epsilon */
 	double alpha_mul;     /* 0.5: backtracking factor */
 	double ftol;          /* 1e-4: sufficient-decrease constant */
-	double wolfe;         /* 0.2: curvature constant */
+	double wolfe;         /* 0.2: curvature constant (g_t.s >= wolfe g.s); <= 0 turns the
+	                         curvature test off */
+	double min_gnorm;     /* stop when ||g|| <= min_gnorm; 0 (default) = off */
 } ccm_cg_params;
 
 typedef struct ccm_cg_result {

@@ -184,16 +184,23 @@ void oracle_calculate_weights(const unsigned char *msa, int L, int N, float thre
 
 /*
  * FP64 host restatement of the device conjugate gradient of
- * ccmpred_b200/csrc/ccm_cg.cu (the optimizer itself is this project's; the
- * reference's libconjugrad is absent, so this is the checker of the device
- * loop, not of libconjugrad).  Same rules: s0 = -g0, alpha0 = 1/||g0||;
- * line search on sufficient decrease (ftol) with safeguarded quadratic
- * backtracking in [0.1, alpha_mul] * alpha, one steepest-descent restart when
- * max_ls trials fail; Polak-Ribiere+ beta with restart when s is not a
- * descent direction; next alpha = 2 (f_old - f_new) / -(g.s_new); stop when
- * (f_{i-k} - f_i)/|f_i| < eps.  f_hist receives f after every iteration
- * (f_hist[0] = f(x0)); returns the status code (0 success, -1023 max
- * iterations, -1022 line search failed).
+ * ccmpred_b200/csrc/ccm_cg.cu with the rules of ccm_cg_rules.cuh (the
+ * optimizer itself is this project's; the reference's libconjugrad is absent,
+ * so this is the checker of the device loop, not of libconjugrad), written
+ * here as a plain loop over FP64 vectors:
+ *   s0 = -g0, alpha0 = 1/||g0||;
+ *   a trial x_t = x + alpha s meets (A) f_t <= f + ftol alpha g.s and
+ *   (C) g_t.s >= wolfe g.s (wolfe <= 0: C always holds);
+ *   A and C, or A with fewer than two trials left: take the step;
+ *   A without C and two trials left: remember alpha, try alpha / alpha_mul;
+ *   not A after such an expansion: retreat to the remembered alpha (taken);
+ *   not A otherwise: safeguarded quadratic backtracking in [0.1, alpha_mul] alpha;
+ *   max_ls trials without a step: restart along -g once (fresh budget), then fail;
+ *   Polak-Ribiere+ beta, steepest descent when s is not a descent direction;
+ *   next alpha = 2 (f_old - f_new) / -(g.s_new) (1/||g|| if that is not positive);
+ *   stop when i >= k and (f_{i-k} - f_i)/|f_i| < eps.
+ * f_hist receives f after every iteration (f_hist[0] = f(x0)); returns the
+ * status code (0 success, -1023 max iterations, -1022 line search failed).
  */
 static double dot(const double *a, const double *b, long n) {
 	double s = 0.0;
@@ -205,7 +212,6 @@ int oracle_conjugrad_f64(const unsigned char *msa, const double *w, int L, int N
 	double lambda_single, double lambda_pair, double *x, int max_iter, int kwin,
 	int max_ls, double alpha_mul, double ftol, double wolfe, double eps,
 	double *f_hist, int *iterations, int *evaluations) {
-	(void)wolfe;
 	const long n = oracle_nvar_padded(L);
 	double *g = (double *)malloc(sizeof(double) * n);
 	double *gt = (double *)malloc(sizeof(double) * n);
@@ -219,41 +225,57 @@ int oracle_conjugrad_f64(const unsigned char *msa, const double *w, int L, int N
 	double gs = -gg;
 	double alpha = 1.0 / sqrt(gg);
 	for (int k = 1; k <= max_iter; k++) {
-		int ok = 0;
-		double ft = 0.0;
-		for (int attempt = 0; attempt < 2 && !ok; attempt++) {
-			for (int ls = 1; ls <= max_ls; ls++) {
-				for (long i = 0; i < n; i++) xt[i] = x[i] + alpha * s[i];
-				ft = oracle_evaluate_f64(msa, w, L, N, lambda_single, lambda_pair, xt, gt);
-				evals++;
-				if (isfinite(ft) && ft <= f + ftol * alpha * gs) { ok = 1; break; }
+		int ok = 0, ls = 0, retreat = 0;
+		double ft = 0.0, good = 0.0;
+		for (;;) {
+			for (long i = 0; i < n; i++) xt[i] = x[i] + alpha * s[i];
+			ft = oracle_evaluate_f64(msa, w, L, N, lambda_single, lambda_pair, xt, gt);
+			evals++;
+			ls++;
+			const int suff = isfinite(ft) && ft <= f + ftol * alpha * gs;
+			const int curv = wolfe <= 0.0 || dot(gt, s, n) >= wolfe * gs;
+			if (retreat) {
+				ok = suff;
+			} else if (suff && (curv || ls + 2 > max_ls)) {
+				ok = 1;
+			} else if (suff) {
+				good = alpha;
+				alpha = alpha / alpha_mul;
+			} else if (good > 0.0) {
+				alpha = good;
+				retreat = 1;
+			} else {
 				double den = 2.0 * (ft - f - gs * alpha);
 				double aq = (isfinite(ft) && den > 0.0) ? -gs * alpha * alpha / den : alpha_mul * alpha;
 				aq = fmin(aq, alpha_mul * alpha);
 				alpha = fmax(aq, 0.1 * alpha);
 			}
-			if (!ok && !steepest) {
+			if (ok) break;
+			if (ls >= max_ls) {
+				if (steepest) break;
 				for (long i = 0; i < n; i++) s[i] = -g[i];
 				gs = -gg;
 				alpha = 1.0 / sqrt(gg);
 				steepest = 1;
-			} else if (!ok) {
-				break;
+				ls = 0;
+				good = 0.0;
+				retreat = 0;
 			}
 		}
 		if (!ok) { status = -1022; break; }
 		double ggnew = dot(gt, gt, n), gtg = dot(gt, g, n), gts_old = dot(gt, s, n);
 		double beta = (ggnew - gtg) / gg;
 		if (!(beta > 0.0)) beta = 0.0;
-		steepest = beta == 0.0;
-		for (long i = 0; i < n; i++) { x[i] = xt[i]; s[i] = beta * s[i] - gt[i]; g[i] = gt[i]; }
 		double gs_new = -ggnew + beta * gts_old;
 		if (!(gs_new < 0.0)) {
-			for (long i = 0; i < n; i++) s[i] = -g[i];
+			beta = 0.0;
 			gs_new = -ggnew;
-			steepest = 1;
 		}
-		alpha = 2.0 * (f - ft) / -gs_new;
+		steepest = beta == 0.0;
+		for (long i = 0; i < n; i++) { x[i] = xt[i]; s[i] = beta * s[i] - gt[i]; g[i] = gt[i]; }
+		double anext = 2.0 * (f - ft) / -gs_new;
+		if (!(anext > 0.0) || !isfinite(anext)) anext = 1.0 / sqrt(ggnew);
+		alpha = anext;
 		gs = gs_new;
 		f = ft;
 		gg = ggnew;

@@ -149,8 +149,11 @@ def oracle_evaluate(msa: np.ndarray, weights: np.ndarray, lambda_single: float,
 
 
 def oracle_conjugrad(msa, weights, lambda_single, lambda_pair, x0, max_iter=250, k=5,
-                     max_ls=5, alpha_mul=0.5, ftol=1e-4, wolfe=0.2, eps=0.01):
-    """FP64 host CG with the rules of the device CG: (x, f_hist, iterations, evals, status)."""
+                     max_ls=5, alpha_mul=0.5, ftol=float(np.float32(1e-4)),
+                     wolfe=float(np.float32(0.2)), eps=0.01):
+    """FP64 host CG with the rules of the device CG: (x, f_hist, iterations, evals, status).
+    The defaults of ftol and wolfe are the reference's float values (src/ccmpred.c:532-533),
+    as the device CG holds them."""
     msa = np.ascontiguousarray(msa, dtype=np.uint8)
     N, L = msa.shape
     w = np.ascontiguousarray(weights, dtype=np.float64)

@@ -1,5 +1,6 @@
 """The C-ABI library loads without a GPU and exports every symbol that
-include/ccmpred_b200.h declares; the ctypes layouts match the header."""
+include/ccmpred_b200.h and include/conjugrad.h declare; the ctypes layouts
+match the headers."""
 import ctypes
 import os
 import re
@@ -8,11 +9,11 @@ import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "ccmpred_b200.h")
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("ccmpred_b200.h", "conjugrad.h")]
 
 
 def declared_functions():
-    text = open(HEADER).read()
+    text = "\n".join(open(h).read() for h in HEADERS)
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     text = re.sub(r"^\s*typedef[^;]*;", "", text, flags=re.M | re.S)
     names = re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_ ]*?[\s\*]+([a-z_][a-z0-9_]*)\s*\(",
@@ -23,7 +24,8 @@ def declared_functions():
 def test_header_declares_the_reference_triple():
     names = declared_functions()
     for n in ("evaluate_cuda", "init_cuda", "destroy_cuda", "ccm_create", "ccm_evaluate",
-              "ccm_calculate_weights", "ccm_destroy"):
+              "ccm_calculate_weights", "ccm_destroy", "conjugrad_init", "conjugrad",
+              "conjugrad_gpu", "conjugrad_malloc", "conjugrad_free"):
         assert n in names
 
 
