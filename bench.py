@@ -91,8 +91,12 @@ def parse_args():
     p.add_argument("--cpu-budget-s", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-precision", action="store_true")
-    p.add_argument("--workload", default="L300_N5000", choices=["L300_N5000", "batch256"],
-                   help="batch256: 256 ragged alignments solved to convergence (MSAs/s)")
+    p.add_argument("--workload", default="L300_N5000",
+                   choices=["L300_N5000", "L1000_N20000", "batch256"],
+                   help="L1000_N20000: 100 CG iterations on the large alignment as one "
+                        "device-side solve (ms/iteration, evals/s); batch256: 256 ragged "
+                        "alignments solved to convergence (MSAs/s)")
+    p.add_argument("--cg-iterations", type=int, default=100)
     p.add_argument("--batch-workers", type=int, default=8)
     p.add_argument("--batch-plain-sample", type=int, default=8)
     p.add_argument("--ref-cuda-steps", type=int, default=3,
@@ -386,12 +390,115 @@ def run_batch(args, world, rank, local):
     }))
 
 
+def run_large(args, world, rank, local):
+    """L=1000, N=20000 (20 % gaps, 30 % near-duplicate rows): GPU reweighting,
+    init_bias, then --cg-iterations CG iterations as ONE device-side solve (line
+    search, direction update and iteration loop in a CUDA graph with conditional
+    nodes; the host waits once), timed with CUDA events on the context stream.
+    The gradient at the final x is checked against the FP64 CUDA-core path."""
+    import ctypes
+
+    import torch
+
+    import ccmpred_b200 as cb
+    from ccmpred_b200 import _lib, synth
+    from ccmpred_b200.host import init_bias
+    torch.cuda.set_device(local)
+    cfg = synth.LARGE_1000x20000
+    msa = synth.generate(cfg)
+    N, L = msa.shape
+    t0 = time.perf_counter()
+    w = cb.calculate_weights(msa, 0.8, device=local)
+    weights_ms = (time.perf_counter() - t0) * 1e3
+    lam2 = float(np.float32(0.2) * np.float32(L - 1))
+    lib = _lib.lib()
+    ev = cb.Evaluator(msa, weights=w, lambda_pair=lam2, path=args.path, device=local)
+    stream = torch.cuda.ExternalStream(ev.stream, device=torch.device("cuda", local))
+    x0 = torch.from_numpy(init_bias(msa)).cuda()
+    g = torch.empty_like(x0)
+    # warm-up: module load, graph construction, a short solve
+    ev.minimize(x0.clone(), max_iterations=2, epsilon=0.0)
+    # one evaluation's kernels (CUDA events per kernel)
+    _lib.check(lib.ccm_profile_begin(ev.handle, 3))
+    for _ in range(3):
+        _lib.check(lib.ccm_evaluate_async(ev.handle, x0.data_ptr(), g.data_ptr(), x0.numel()))
+    kms = (ctypes.c_double * 8)()
+    nk, ne = ctypes.c_int(0), ctypes.c_int(0)
+    _lib.check(lib.ccm_profile_end(ev.handle, kms, 8, ctypes.byref(nk), ctypes.byref(ne)))
+    names = ["prep", "forward", "backward", "finalize"]
+    kernels = {names[i]: kms[i] / max(ne.value, 1) for i in range(min(nk.value, 4))}
+    torch.cuda.synchronize()
+    xs = x0.clone()
+    launches0 = lib.ccm_launch_count(ev.handle)
+    sampler = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    res = ev.minimize(xs, max_iterations=args.cg_iterations, epsilon=0.0)
+    b.record(stream)
+    b.synchronize()
+    clocks = sampler.stop()
+    elapsed_ms = max_over_ranks(world, a.elapsed_time(b))
+    launches = lib.ccm_launch_count(ev.handle) - launches0
+    if rank != 0:
+        ev.close()
+        return
+    # the gradient at the final x against the FP64 CUDA-core path
+    f_tc = ev.evaluate(xs, g)
+    g_tc = g.double().cpu().numpy()
+    ev.close()
+    with cb.Evaluator(msa, weights=w, lambda_pair=lam2, path="simt_f64", device=local) as r64:
+        g64 = torch.empty_like(xs, dtype=torch.float64)
+        f64 = r64.evaluate(xs.double(), g64)
+        g64 = g64.cpu().numpy()
+    nrm = np.linalg.norm
+    peaks, peak_kind = measured_peaks()
+    peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
+    flops_eval = 4.0 * N * (21 * L) ** 2
+    achieved = flops_eval * res.evaluations / (elapsed_ms / 1e3) / 1e12
+    its = max(res.iterations, 1)
+    emit({
+        "metric": f"CG iterations/s at L=1000 N=20000 ({args.cg_iterations} iterations, one "
+                  "device-side solve)",
+        "value": res.iterations / (elapsed_ms / 1e3), "unit": "iterations/s", "n_gpus": world,
+        "higher_is_better": True, "scaling": "weak", "data": "synthetic",
+        "dtype": PATH_DTYPE[args.path],
+        "config": {"workload": "L1000_N20000", "ncol": L, "nrow": N, "gap_frac": cfg.gap_frac,
+                   "dup_frac": cfg.dup_frac, "seed": cfg.seed, "path": args.path,
+                   "cg": f"{args.cg_iterations} iterations, epsilon 0 (no early stop), "
+                         "max_linesearch 5, ftol 1e-4, wolfe 0.2 (float values)"},
+        "ms_per_iteration": elapsed_ms / its, "solve_ms": elapsed_ms,
+        "iterations": res.iterations, "evaluations": res.evaluations,
+        "evals_per_s": res.evaluations / (elapsed_ms / 1e3), "cg_status": res.status,
+        "kernels_ms_per_evaluation": kernels,
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "peak_source": f"{peak_kind} bf16_tflops_sustained",
+                     "flops_per_evaluation": flops_eval,
+                     "note": "useful FLOPs of both contractions per evaluation over the whole "
+                             "solve's time (CG vector passes and graph overhead included)"},
+        "precision_at_final_x": {
+            "f_rel": abs(f_tc - f64) / abs(f64),
+            "g_rel": float(nrm(g_tc - g64) / nrm(g64)),
+            "reference": "FP64 CUDA-core path (simt_f64) at the same x"},
+        "gpu_launches": int(launches), "clocks": clocks,
+        "init_ms": {"weights": weights_ms},
+        "cpu_baseline": None,
+    })
+
+
 def main():
     args = parse_args()
     quiet_stdout()
     world, rank, local = dist_init(args)
     if args.impl == "b200" and args.workload == "batch256":
         run_batch(args, world, rank, local)
+        barrier(world)
+        return
+    if args.impl == "b200" and args.workload == "L1000_N20000":
+        run_large(args, world, rank, local)
         barrier(world)
         return
     if args.impl == "reference":

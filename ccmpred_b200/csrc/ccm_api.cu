@@ -279,18 +279,25 @@ int alloc_tc(ccm_context *c) {
     std::memset(&c->i8bwd_maps, 0, sizeof(c->i8bwd_maps));
     if ((rc = make_map_u8(&c->i8fwd_maps.a1, c->d_o1, Np, S, 64, 128)) != CCM_OK) return rc;
     if ((rc = make_map_u8(&c->i8fwd_maps.a128, c->d_o128, Np, S, 64, 128)) != CCM_OK) return rc;
-    if ((rc = make_map_u8(&c->i8bwd_maps.o1, c->d_o1, Np, S, 128, 32)) != CCM_OK) return rc;
-    if ((rc = make_map_u8(&c->i8bwd_maps.o128, c->d_o128, Np, S, 128, 32)) != CCM_OK) return rc;
+    // backward operands: the dense path reads 128-slot x 32-row boxes of the
+    // row-major matrices (128-byte swizzle); the sparse path stores them tiled
+    // (4 KB shared-memory images, swizzle applied) and reads 16 rows of 256 bytes
+    const long long trows = (long long)Np * S / 256;
+    const int none = CU_TENSOR_MAP_SWIZZLE_NONE;
+    auto bwd_map = [&](CUtensorMap *m, void *p) {
+      return sp ? make_map_u8(m, p, trows, 256, 256, 16, none) : make_map_u8(m, p, Np, S, 128, 32);
+    };
+    if ((rc = bwd_map(&c->i8bwd_maps.o1, c->d_o1)) != CCM_OK) return rc;
+    if ((rc = bwd_map(&c->i8bwd_maps.o128, c->d_o128)) != CCM_OK) return rc;
     for (int i = 0; i < 3; ++i) {
       if (!sp && (rc = make_map_u8(&c->i8fwd_maps.b[i], c->d_wdig[i], S, S, 128, 64)) != CCM_OK)
         return rc;
-      if ((rc = make_map_u8(&c->i8bwd_maps.r[i], c->d_rdig[i], Np, S, 128, 32)) != CCM_OK) return rc;
+      if ((rc = bwd_map(&c->i8bwd_maps.r[i], c->d_rdig[i])) != CCM_OK) return rc;
     }
     if (sp) {
       std::memset(&c->i8sp_maps, 0, sizeof(c->i8sp_maps));
       // tiled operand storage viewed as rows of 256 bytes; one box = one stage tile
       const long long KP = c->KP;
-      const int none = CU_TENSOR_MAP_SWIZZLE_NONE;
       if ((rc = make_map_u8(&c->i8sp_maps.a1, c->d_ac1, Np * KP / 512, 256, 256, 32, none)) !=
               CCM_OK ||
           (rc = make_map_u8(&c->i8sp_maps.a128, c->d_ac128, Np * KP / 512, 256, 256, 32, none)) !=

@@ -253,15 +253,29 @@ __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ 
   }
 }
 
+// Tiled storage of the backward's operands on the sparse path (one-hot x1 /
+// x128 and the digits of R, Npad x S bytes each): the 32-row x 128-slot tile
+// (kb = n / 32, sb = s / 128) that one pipeline stage of one CTA reads is stored
+// contiguously (4 KB) as the shared-memory image the MMA reads -- rows of 128
+// slots, 16-byte chunk c of row r at chunk c ^ (r & 7) (128-byte swizzle) --
+// tiles in the order sb * KB + kb, KB = Npad / 32.  One TMA box of 16 rows of
+// 256 bytes moves a tile (twice the bytes per TMA row request of a 128-slot box
+// of the row-major matrix).
+__host__ __device__ constexpr long long i8_bwd_tile_offset(int n, int s, int KB) {
+  return ((long long)(s >> 7) * KB + (n >> 5)) * 4096 + (n & 31) * 128 +
+         (((((s & 127) >> 4) ^ (n & 7)) & 7) << 4) + (s & 15);
+}
+
 // One-hot operands of the integer path (slot groups G): O1[n][s] = 1 and
 // O128[n][s] = 128 where the state of column l(s) in row n is q(s), and in the
-// ones slot of every real row; 0 elsewhere.
-template <class G>
+// ones slot of every real row; 0 elsewhere.  TILED: stored as i8_bwd_tile_offset.
+template <class G, bool TILED>
 __global__ void i8_onehot_kernel(const uint8_t *__restrict__ msa, uint8_t *__restrict__ o1,
                                  uint8_t *__restrict__ o128, int L, int N, int S, int Npad) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long long)Npad * S) return;
   const int n = (int)(idx / S), s = (int)(idx % S);
+  const long long at = TILED ? i8_bwd_tile_offset(n, s, Npad >> 5) : idx;
   const int t = s / G::kSlots, r = s % G::kSlots;
   bool one = false;
   if (n < N) {
@@ -272,8 +286,8 @@ __global__ void i8_onehot_kernel(const uint8_t *__restrict__ msa, uint8_t *__res
       one = l < L && msa[(long long)n * L + l] == q;
     }
   }
-  o1[idx] = one ? 1 : 0;
-  o128[idx] = one ? 128 : 0;
+  o1[at] = one ? 1 : 0;
+  o128[at] = one ? 128 : 0;
 }
 
 }  // namespace ccm
@@ -321,8 +335,9 @@ struct I8FwdSmem {
 // merge -- the half's first 32-column chunk into a TMEM stash that no MMA writes
 // (t_stash), the other chunks into registers -- and the arrival on `lo_bar` after
 // the merge then releases both accumulators, so that the next tile's MMAs run
-// during passes B and C.
-template <class G, int H, bool REGS = false>
+// during passes B and C.  TILED: the digits of R go to the backward's tiled
+// storage (i8_bwd_tile_offset) instead of row-major Npad x S.
+template <class G, int H, bool REGS = false, bool TILED = false>
 __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint32_t t_hi,
                                                      uint32_t t_lo, const float *tab_scale,
                                                      const float *tab_v, float *xbuf, int q,
@@ -500,7 +515,24 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
       w1[e4] = pack(qv[0] >> 7, qv[1] >> 7, qv[2] >> 7, qv[3] >> 7) & 0x7F7F7F7Fu;
       w2[e4] = pack(qv[0], qv[1], qv[2], qv[3]) & 0x7F7F7F7Fu;
     }
-    const long long off = rbase + cc * 32;
+    long long off = rbase + cc * 32;
+    if constexpr (TILED) {
+      // the 32 slots [s0, s0 + 32) of row n are 16-byte chunks c, c + 1 (c even) of
+      // the tile row; swizzled to c ^ m and (c ^ m) ^ 1, m = n & 7: one aligned
+      // 32-byte pair, its halves exchanged when m is odd
+      const int s0 = t * G::kSlots + cc * 32;
+      const int m = n & 7, c = (s0 & 127) >> 4;
+      off = ((long long)(s0 >> 7) * (args.Npad >> 5) + (n >> 5)) * 4096 + (n & 31) * 128 +
+            (((c ^ m) & 6) << 4);
+      if (m & 1) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          uint32_t v = w0[i]; w0[i] = w0[i + 4]; w0[i + 4] = v;
+          v = w1[i]; w1[i] = w1[i + 4]; w1[i + 4] = v;
+          v = w2[i]; w2[i] = w2[i + 4]; w2[i + 4] = v;
+        }
+      }
+    }
     st_global_v8(args.r[0] + off, w0);
     st_global_v8(args.r[1] + off, w1);
     st_global_v8(args.r[2] + off, w2);
@@ -982,11 +1014,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
       const long long part = (long long)tile * 2 + rank;
       // both accumulators are released inside, right after the merge
       if (half == 0)
-        i8_fwd_epilogue_tile<Groups192, 0, true>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v,
+        i8_fwd_epilogue_tile<Groups192, 0, true, true>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v,
                                                  xbuf, q, lane, n, t, part, empty_bar,
                                                  t_stash + lq);
       else
-        i8_fwd_epilogue_tile<Groups192, 1, true>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v,
+        i8_fwd_epilogue_tile<Groups192, 1, true, true>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v,
                                                  xbuf, q, lane, n, t, part, empty_bar,
                                                  t_stash + 32 + lq);
     }
@@ -1029,7 +1061,9 @@ struct I8BwdSmem {
   static constexpr int kTotal = kTOff + kTBytes + 1024;
 };
 
-template <bool SYM, class G>
+// TILED: the operands are in the tiled storage of i8_bwd_tile_offset (the sparse
+// path); else row-major Npad x S.  The shared-memory images are the same.
+template <bool SYM, class G, bool TILED>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
     i8_backward_kernel(const __grid_constant__ I8BwdMaps maps, BwdArgs args) {
   using SM = I8BwdSmem;
@@ -1088,20 +1122,25 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
             break;
           }
           uint8_t *st = smem + stage * SM::kStage;
+          // row-major: box (slot x, row y); tiled: the 4 KB tile of (slot block,
+          // K block) is 16 rows of 256 bytes at row 16 * (sb * KB + kb)
           const int y = kb * kI8BwdBK;
+          const int xp = TILED ? 0 : xP, xq = TILED ? 0 : xQ;
+          const int yp = TILED ? ((xP >> 7) * k_blocks + kb) * 16 : y;
+          const int yq = TILED ? ((xQ >> 7) * k_blocks + kb) * 16 : y;
           const uint32_t fb = mapa_shared(smem_u32(&full[stage]), 0);
           if (rank == 0) mbar_arrive_expect_tx(&full[stage], 2 * (SYM ? 10 : 5) * SM::kTile);
-          tma_load_2d_pair(st + 0 * SM::kTile, &maps.o1, fb, xP, y);
-          tma_load_2d_pair(st + 1 * SM::kTile, &maps.o128, fb, xP, y);
+          tma_load_2d_pair(st + 0 * SM::kTile, &maps.o1, fb, xp, yp);
+          tma_load_2d_pair(st + 1 * SM::kTile, &maps.o128, fb, xp, yp);
           if (SYM)
             for (int i = 0; i < 3; ++i)
-              tma_load_2d_pair(st + (2 + i) * SM::kTile, &maps.r[i], fb, xP, y);
+              tma_load_2d_pair(st + (2 + i) * SM::kTile, &maps.r[i], fb, xp, yp);
           if (SYM) {
-            tma_load_2d_pair(st + 5 * SM::kTile, &maps.o1, fb, xQ, y);
-            tma_load_2d_pair(st + 6 * SM::kTile, &maps.o128, fb, xQ, y);
+            tma_load_2d_pair(st + 5 * SM::kTile, &maps.o1, fb, xq, yq);
+            tma_load_2d_pair(st + 6 * SM::kTile, &maps.o128, fb, xq, yq);
           }
           for (int i = 0; i < 3; ++i)
-            tma_load_2d_pair(st + (7 + i) * SM::kTile, &maps.r[i], fb, xQ, y);
+            tma_load_2d_pair(st + (7 + i) * SM::kTile, &maps.r[i], fb, xq, yq);
         }
       }
       const uint32_t issued = it;
@@ -1349,16 +1388,16 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   const bool sym = c->gradient != CCM_GRADIENT_PARTIAL;
   const dim3 bgrid(2 * bpairs);
   if (sp && sym)
-    i8_backward_kernel<true, Groups192>
+    i8_backward_kernel<true, Groups192, true>
         <<<bgrid, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
   else if (sp)
-    i8_backward_kernel<false, Groups192>
+    i8_backward_kernel<false, Groups192, true>
         <<<bgrid, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
   else if (sym)
-    i8_backward_kernel<true, Groups256>
+    i8_backward_kernel<true, Groups256, false>
         <<<bgrid, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
   else
-    i8_backward_kernel<false, Groups256>
+    i8_backward_kernel<false, Groups256, false>
         <<<bgrid, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
   prof_mark(c);
 
@@ -1383,14 +1422,14 @@ cudaError_t i8_configure_kernels() {
       (e = cudaFuncSetAttribute(i8sp_forward_kernel, (cudaFuncAttribute)kMax, I8SpSmem::kTotal)) !=
           cudaSuccess)
     return e;
-  if ((e = cudaFuncSetAttribute(i8_backward_kernel<true, Groups256>, (cudaFuncAttribute)kMax,
+  if ((e = cudaFuncSetAttribute(i8_backward_kernel<true, Groups256, false>, (cudaFuncAttribute)kMax,
                                 I8BwdSmem::kTotal)) != cudaSuccess ||
-      (e = cudaFuncSetAttribute(i8_backward_kernel<false, Groups256>, (cudaFuncAttribute)kMax,
+      (e = cudaFuncSetAttribute(i8_backward_kernel<false, Groups256, false>, (cudaFuncAttribute)kMax,
                                 I8BwdSmem::kTotal)) != cudaSuccess ||
-      (e = cudaFuncSetAttribute(i8_backward_kernel<true, Groups192>, (cudaFuncAttribute)kMax,
+      (e = cudaFuncSetAttribute(i8_backward_kernel<true, Groups192, true>, (cudaFuncAttribute)kMax,
                                 I8BwdSmem::kTotal)) != cudaSuccess)
     return e;
-  return cudaFuncSetAttribute(i8_backward_kernel<false, Groups192>, (cudaFuncAttribute)kMax,
+  return cudaFuncSetAttribute(i8_backward_kernel<false, Groups192, true>, (cudaFuncAttribute)kMax,
                               I8BwdSmem::kTotal);
 }
 
@@ -1418,7 +1457,7 @@ cudaError_t i8_backward_max_pairs(int *pairs) {
   cfg.blockDim = dim3(kI8Threads, 1, 1);
   cfg.dynamicSmemBytes = I8BwdSmem::kTotal;
   *pairs = 0;
-  return cudaOccupancyMaxActiveClusters(pairs, i8_backward_kernel<true, Groups256>, &cfg);
+  return cudaOccupancyMaxActiveClusters(pairs, i8_backward_kernel<true, Groups256, false>, &cfg);
 }
 
 // One-hot operands for a context of the integer paths (Npad x S bytes each), and
@@ -1427,11 +1466,12 @@ cudaError_t i8_build_onehot(ccm_context *c) {
   const long long total = (long long)c->Npad * c->S;
   const unsigned grid = (unsigned)((total + 255) / 256);
   if (c->path != CCM_PATH_TC_I8SP) {
-    i8_onehot_kernel<Groups256><<<grid, 256, 0, c->stream>>>(c->d_msa, c->d_o1, c->d_o128, c->L,
+    i8_onehot_kernel<Groups256, false><<<grid, 256, 0, c->stream>>>(c->d_msa, c->d_o1, c->d_o128, c->L,
                                                              c->N, c->S, c->Npad);
     return cudaGetLastError();
   }
-  i8_onehot_kernel<Groups192><<<grid, 256, 0, c->stream>>>(c->d_msa, c->d_o1, c->d_o128, c->L,
+  // the sparse path's backward reads its operands from tiled storage
+  i8_onehot_kernel<Groups192, true><<<grid, 256, 0, c->stream>>>(c->d_msa, c->d_o1, c->d_o128, c->L,
                                                            c->N, c->S, c->Npad);
   const long long bytes = (long long)c->Npad * (c->KP / 8);
   i8sp_onehot_kernel<<<(unsigned)((bytes + 255) / 256), 256, 0, c->stream>>>(

@@ -54,6 +54,17 @@ def sp_b_index(KP, SW):
              + ((((xx >> 4) ^ (r >> 2)) & 1) << 4) + (xx & 15)))
 
 
+def sp_bwd_index(Npad, S):
+    """The backward's operands (one-hot x1 / x128, digits of R), Npad x S: 32-row x
+    128-slot tiles (kb = n // 32, sb = s // 128) of 4 KB in the order sb * KB + kb,
+    KB = Npad // 32; rows of 128 slots, 16-byte chunk c of row r at chunk c ^ (r & 7)."""
+    n = np.arange(Npad)[:, None]
+    s = np.arange(S)[None, :]
+    KB = Npad // 32
+    return (((s >> 7) * KB + (n >> 5)) * 4096 + (n & 31) * 128
+            + (((((s & 127) >> 4) ^ (n & 7)) & 7) << 4) + (s & 15))
+
+
 def onehot_natural(msa, KP, Npad):
     """O[n][l * 21 + q] = 1 where column l of row n holds state q."""
     N, L = msa.shape

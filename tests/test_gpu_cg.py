@@ -93,3 +93,34 @@ def test_cg_result_is_the_evaluation_at_the_returned_x(gpu, path):
         assert f == res.fx
         assert abs(float(torch.linalg.vector_norm(g.double())) - res.gnorm) <= 1e-12 * res.gnorm
     ev.close()
+
+
+@pytest.mark.parametrize("path", ["tc_i8sp", "tc_bf16x2", "simt_f32"])
+def test_whole_solve_graph_equals_per_iteration_loop(gpu, oracle_mod, path):
+    """Without a progress callback the whole solve is one graph launch (line
+    search, direction update and stopping test on the device, in conditional
+    nodes); with one, the host launches one line-search graph per iteration.
+    Both apply the same kernels and rules: the same x bit for bit, the same
+    iterations and evaluations, and the trajectory of the FP64 restatement."""
+    import torch
+    msa = synth.generate(synth.MSAConfig("cgw", 30, 400, n_pairs=4, dup_frac=0.2, seed=64))
+    N, L = msa.shape
+    w = oracle_mod.oracle_weights(msa, 0.8)
+    lam1, lam2 = 0.01, 0.2 * (L - 1)
+    x0 = init_bias(msa)
+    ev = Evaluator(msa, weights=w, lambda_single=lam1, lambda_pair=lam2, path=path)
+    xa = torch.from_numpy(x0.copy()).cuda()
+    ra = ev.minimize(xa, max_iterations=40, epsilon=1e-3)
+    xb = torch.from_numpy(x0.copy()).cuda()
+    seen = []
+    rb = ev.minimize(xb, max_iterations=40, epsilon=1e-3,
+                     progress=lambda k, ls, fx, xn, gn, st: seen.append(k) and False)
+    ev.close()
+    assert torch.equal(xa, xb)
+    assert (ra.status, ra.iterations, ra.evaluations, ra.fx) == \
+        (rb.status, rb.iterations, rb.evaluations, rb.fx)
+    assert seen == list(range(1, rb.iterations + 1))
+    _, fh, it_h, ev_h, st_h = oracle_mod.oracle_conjugrad(msa, w, lam1, lam2, x0.astype(np.float64),
+                                                          max_iter=40, eps=1e-3)
+    assert ra.status == st_h and ra.iterations == it_h and ra.evaluations == ev_h
+    assert abs(ra.fx - fh[-1]) / abs(fh[-1]) < 2e-5

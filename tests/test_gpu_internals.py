@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from ccmpred_b200 import Evaluator, lib, synth
-from sparse_layout import slot192, sp_a_index, sp_b_index, sp_e_index
+from sparse_layout import slot192, sp_a_index, sp_b_index, sp_bwd_index, sp_e_index
 
 pytestmark = pytest.mark.gpu
 
@@ -216,8 +216,11 @@ def test_sparse_integer_path_stages(gpu, L, N, seed):
         onehot_nat[np.arange(N), l * Q + msa[:, l].astype(np.int64)] = 1
     assert np.array_equal(logical.reshape(Npad, KP), onehot_nat)
 
-    # one-hot of the backward in 192-slot groups, ones slot 189
-    O1 = fetch(ev, 0, np.uint8).reshape(Npad, S)
+    # one-hot of the backward in 192-slot groups, ones slot 189, read through the
+    # backward's tiled storage
+    bwd = sp_bwd_index(Npad, S)
+    assert np.array_equal(np.sort(bwd.ravel()), np.arange(Npad * S))
+    O1 = fetch(ev, 0, np.uint8)[bwd]
     O = np.zeros((Npad, S), dtype=np.uint8)
     for n in range(N):
         for l in range(L):
@@ -247,7 +250,7 @@ def test_sparse_integer_path_stages(gpu, L, N, seed):
     for l in range(L):
         Onat[np.arange(N), msa[:, l].astype(np.int64) * L + l] = 1.0    # column b*L + k
     logits = (Onat @ Wdeq).reshape(N, Q, L)                             # [n, a, j]
-    r = [fetch(ev, 4 + i, np.uint8).reshape(Npad, S) for i in range(3)]
+    r = [fetch(ev, 4 + i, np.uint8)[bwd] for i in range(3)]
     R_gpu = digits_value(*r) / 2.0**21
     R_exp = np.zeros((Npad, S))
     for l in range(L):

@@ -7,7 +7,7 @@ import pytest
 
 from ccmpred_b200 import synth
 from sparse_layout import (Q, compress_2to4, decompress_2to4, onehot_natural, slot192,
-                           sp_a_index, sp_b_index, sp_e_index, sp_shapes)
+                           sp_a_index, sp_b_index, sp_bwd_index, sp_e_index, sp_shapes)
 
 
 def adversarial_msa(L, N, seed):
@@ -42,8 +42,23 @@ def test_groups192_slots(L):
 
 @pytest.mark.parametrize("L,N", [(1, 9), (13, 50), (40, 300), (300, 5000)])
 def test_tiled_stores_are_bijections(L, N):
-    _, SW, _, KP, Npad = sp_shapes(L, N)
+    _, SW, S, KP, Npad = sp_shapes(L, N)
     for idx, size in ((sp_a_index(Npad, KP), Npad * KP // 2), (sp_e_index(Npad, KP), Npad * KP // 8),
-                      (sp_b_index(KP, SW), KP * SW)):
+                      (sp_b_index(KP, SW), KP * SW), (sp_bwd_index(Npad, S), Npad * S)):
         assert idx.size == size
         assert np.array_equal(np.sort(idx.ravel()), np.arange(size))
+
+
+def test_backward_tile_rows_are_aligned_32_byte_pairs():
+    """The forward epilogue writes 32 consecutive slots of one row of R as one
+    32-byte store: in the backward's tiled storage those bytes form one aligned
+    32-byte pair of 16-byte chunks (halves exchanged on odd rows mod 8)."""
+    Npad, S = 512, 768
+    idx = sp_bwd_index(Npad, S)
+    for n in range(0, Npad, 7):
+        for s0 in range(0, S, 32):
+            b = idx[n, s0:s0 + 32]
+            base = b.min()
+            assert base % 32 == 0 and b.max() == base + 31
+            lo_first = b[0] == base
+            assert lo_first == ((n & 7) % 2 == 0)
