@@ -58,9 +58,13 @@ def calculate_weights(msa: np.ndarray, threshold: float = 0.8, device: int = 0) 
 
 def solve_batch(msas, workers: int = 8, path: str = "tc_i8sp", threshold: float = 0.8,
                 max_iterations: int = 250, epsilon: float = 0.01, contact_maps: bool = True,
-                device: int = 0, sms_per_worker: int = 0):
+                device: int = 0, sms_per_worker: int = 0, waves: bool = True,
+                wave_max: int = 64, wave_bytes: int = 0):
     """Solve many alignments to convergence concurrently (ccm_solve_batch).
 
+    ``waves`` (default): one graph launch per wave of alignments (``wave_max``
+    alignments at most, ``wave_bytes`` of device memory, 0 = 60 % of the free
+    memory); else ``workers`` host threads with a context and stream each.
     Returns (results, maps): per-alignment CcmBatchResult and APC contact maps."""
     arrs = [np.ascontiguousarray(m, dtype=np.uint8) for m in msas]
     n = len(arrs)
@@ -72,6 +76,7 @@ def solve_batch(msas, workers: int = 8, path: str = "tc_i8sp", threshold: float 
     lib().ccm_batch_params_default(ctypes.byref(p))
     p.workers, p.path, p.reweighting_threshold, p.device = workers, PATHS[path], threshold, device
     p.sms_per_worker = sms_per_worker
+    p.waves, p.wave_max, p.wave_bytes = int(bool(waves)), wave_max, wave_bytes
     p.cg.max_iterations, p.cg.epsilon = max_iterations, epsilon
     res = (_lib.CcmBatchResult * max(n, 1))()
     maps = [np.empty((a.shape[1], a.shape[1]), dtype=np.float32) for a in arrs] if contact_maps else None

@@ -85,7 +85,9 @@ class CcmBatchParams(ctypes.Structure):
     _fields_ = [("reweighting_threshold", ctypes.c_float), ("lambda_single", ctypes.c_float),
                 ("lambda_pair_factor", ctypes.c_float), ("path", ctypes.c_int),
                 ("workers", ctypes.c_int), ("device", ctypes.c_int), ("use_apc", ctypes.c_int),
-                ("sms_per_worker", ctypes.c_int), ("cg", CcmCgParams)]
+                ("sms_per_worker", ctypes.c_int), ("waves", ctypes.c_int),
+                ("wave_max", ctypes.c_int), ("wave_bytes", ctypes.c_size_t),
+                ("cg", CcmCgParams)]
 
 
 class CcmBatchResult(ctypes.Structure):

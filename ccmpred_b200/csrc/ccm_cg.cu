@@ -134,10 +134,14 @@ struct CgHandles {
 };
 
 // After the initial evaluation: f0 (from the evaluation record, or from f_slot
-// when a callback evaluated), g0.g0 from the partials.
+// when a callback evaluated), g0.g0 from the partials.  In a graph (set_out) it
+// also sets the value of the solve's outer WHILE node: no iteration when x0 is
+// already a minimum or f0 is not finite.
 __global__ void __launch_bounds__(256) cg_start_kernel(CgCtl *ctl, const double *part,
                                                        int nblocks, const ccm_result *res,
-                                                       const double *f_slot) {
+                                                       const double *f_slot,
+                                                       cudaGraphConditionalHandle h_out,
+                                                       int set_out) {
   __shared__ double red[8];
   const double gg = reduce_part(part, nblocks, 1, red);
   if (threadIdx.x == 0) {
@@ -146,7 +150,18 @@ __global__ void __launch_bounds__(256) cg_start_kernel(CgCtl *ctl, const double 
       ctl->status = CCM_ERR_DEVICE;
       ctl->ls_active = 0;
     }
+    if (set_out) cudaGraphSetConditional(h_out, ctl->status == kCgRunning ? 1u : 0u);
   }
+}
+
+// The solve's x ends in the trial buffer when the last accepted step had parity
+// 0: copy it to the caller's buffer (a no-op otherwise).
+__global__ void cg_final_x_kernel(const CgCtl *__restrict__ ctl, const float *__restrict__ x1,
+                                  float *__restrict__ x0, long long n) {
+  if (ctl->parity != 1) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x0[i] = x1[i];
 }
 
 __global__ void __launch_bounds__(256) cg_control_kernel(CgCtl *ctl, CgRuleParams p,
@@ -316,16 +331,23 @@ int capture_readback(CgRun &r, cudaGraph_t graph, cudaGraphNode_t dep) {
   return CCM_OK;
 }
 
-// Whole solve: WHILE(outer) { WHILE(ls0) { trial parity 0 }; IF(it2) { WHILE(ls1)
-// { trial parity 1 } } }, then the read-back.
-int build_solve_graph(CgRun &r, const CgRuleParams &rp) {
-  cudaGraph_t g = nullptr;
-  cudaError_t e = cudaGraphCreate(&g, 0);
-  if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "cg graph: %s", cudaGetErrorString(e));
-  cudaGraphConditionalHandle h_out, h_ls0, h_it2, h_ls1;
-  cudaGraphNode_t n_out, n_ls0, n_it2, n_ls1;
-  cudaGraph_t b_out, b_ls0, b_it2, b_ls1;
-  e = add_conditional(g, cudaGraphCondTypeWhile, 1, nullptr, 0, &h_out, &n_out, &b_out);
+// The iteration loop of a whole solve, added to `g` after `deps`:
+// WHILE(outer) { WHILE(ls0) { trial parity 0 }; IF(it2) { WHILE(ls1) { trial
+// parity 1 } } }.  The outer WHILE node's handle h_out exists already (a kernel
+// before the loop may set it).
+int add_solve_loop(CgRun &r, const CgRuleParams &rp, cudaGraph_t g,
+                   cudaGraphConditionalHandle h_out, const cudaGraphNode_t *deps, size_t ndeps,
+                   cudaGraphNode_t *n_out) {
+  cudaGraphConditionalHandle h_ls0, h_it2, h_ls1;
+  cudaGraphNode_t n_ls0, n_it2, n_ls1;
+  cudaGraph_t b_out = nullptr, b_ls0, b_it2, b_ls1;
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h_out;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaError_t e = cudaGraphAddNode(n_out, g, deps, ndeps, &np);
+  if (e == cudaSuccess) b_out = np.conditional.phGraph_out[0];
   if (e == cudaSuccess)
     e = add_conditional(b_out, cudaGraphCondTypeWhile, 1, nullptr, 0, &h_ls0, &n_ls0, &b_ls0);
   if (e == cudaSuccess)
@@ -336,6 +358,21 @@ int build_solve_graph(CgRun &r, const CgRuleParams &rp) {
   if (e != cudaSuccess) rc = set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
   if (rc == CCM_OK) rc = capture_trial_into(r, b_ls0, 0, rp, CgHandles{h_ls0, h_ls1, h_it2, h_out, 2, 0});
   if (rc == CCM_OK) rc = capture_trial_into(r, b_ls1, 1, rp, CgHandles{h_ls1, h_ls0, h_it2, h_out, 2, 1});
+  return rc;
+}
+
+// Whole solve after the initial evaluation (on the host's stream): the loop,
+// then the read-back.
+int build_solve_graph(CgRun &r, const CgRuleParams &rp) {
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaGraphCreate(&g, 0);
+  if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "cg graph: %s", cudaGetErrorString(e));
+  cudaGraphConditionalHandle h_out;
+  cudaGraphNode_t n_out = nullptr;
+  e = cudaGraphConditionalHandleCreate(&h_out, g, 1, cudaGraphCondAssignDefault);
+  int rc = e == cudaSuccess ? CCM_OK
+                            : set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
+  if (rc == CCM_OK) rc = add_solve_loop(r, rp, g, h_out, nullptr, 0, &n_out);
   if (rc == CCM_OK) rc = capture_readback(r, g, n_out);
   if (rc == CCM_OK) {
     e = cudaGraphInstantiate(&r.exec[0], g, 0);
@@ -391,6 +428,122 @@ int finish(CgRun &r, float *d_x, ccm_cg_result *result, int stopped) {
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------- solves in a shared graph
+// The batch solver puts the solves of many alignments into one graph: each one
+// a chain initial evaluation -> start -> outer WHILE -> final x -> read-back,
+// with no edge between alignments, so the graph's independent branches run
+// concurrently.  All captures go through the context's stream.
+struct ccm::CgGraphSolve {
+  CgRun r;
+};
+
+int ccm::cg_graph_solve_add(ccm_context *c, float *d_x, const ccm_cg_params *params,
+                            cudaGraph_t graph, CgGraphSolve **out, cudaGraphNode_t *last) {
+  *out = nullptr;
+  int rc = check_params(params, "ccm_solve_batch");
+  if (rc != CCM_OK) return rc;
+  if (c->path == CCM_PATH_SIMT_F64)
+    return set_last_error(CCM_ERR_INVALID, "ccm_solve_batch: needs a float evaluation path");
+  const CgRuleParams rp = rule_params(*params);
+  CgGraphSolve *gs = new CgGraphSolve();
+  CgRun &r = gs->r;
+  r.c = c;
+  r.n = c->nvarp;
+  r.xb[0] = d_x;
+  r.fused = c->path == CCM_PATH_TC_BF16X2 || c->path == CCM_PATH_TC_BF16X3 ||
+            c->path == CCM_PATH_TC_I8X3 || c->path == CCM_PATH_TC_I8SP;
+  const size_t bytes = sizeof(float) * (size_t)r.n;
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&r.xb[1]), bytes));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&r.gb[0]), bytes));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&r.gb[1]), bytes));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&r.s), bytes));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&r.d_ctl), sizeof(CgCtl)));
+  chk(dev_alloc_raw(c, reinterpret_cast<void **>(&r.d_part), sizeof(double) * 6 * kDotBlocks));
+  r.h_ctl = static_cast<CgCtl *>(pinned_small_alloc(kCgCtlHead));
+  if (!r.h_ctl) chk(cudaErrorMemoryAllocation);
+  if (e != cudaSuccess) {
+    free_run(r);
+    delete gs;
+    (void)cudaGetLastError();
+    return set_last_error(e == cudaErrorMemoryAllocation ? CCM_ERR_NOMEM : CCM_ERR_CUDA,
+                          "ccm_solve_batch: %s", cudaGetErrorString(e));
+  }
+  const bool prof = c->prof_on;
+  c->prof_on = false;
+  cudaStream_t s = c->stream;
+  cudaGraphConditionalHandle h_out;
+  e = cudaGraphConditionalHandleCreate(&h_out, graph, 1, cudaGraphCondAssignDefault);
+  std::vector<cudaGraphNode_t> front;
+  // initial evaluation, g0.g0, start (which sets the outer loop's value)
+  if (e == cudaSuccess)
+    e = cudaStreamBeginCaptureToGraph(s, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    rc = enqueue_evaluation(c, r.xb[0], r.gb[0]);
+    cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(r.gb[0], nullptr, nullptr, r.n, r.d_part);
+    cg_start_kernel<<<1, 256, 0, s>>>(r.d_ctl, r.d_part, kDotBlocks, c->d_out, nullptr, h_out, 1);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    if (cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &nd) == cudaSuccess)
+      front.assign(deps, deps + nd);
+    cudaGraph_t tmp = nullptr;
+    e = cudaStreamEndCapture(s, &tmp);
+  }
+  cudaGraphNode_t n_out = nullptr;
+  if (e != cudaSuccess && rc == CCM_OK)
+    rc = set_last_error(CCM_ERR_CUDA, "ccm_solve_batch: %s", cudaGetErrorString(e));
+  if (rc == CCM_OK && front.empty()) rc = set_last_error(CCM_ERR_CUDA, "ccm_solve_batch: capture");
+  if (rc == CCM_OK) rc = add_solve_loop(r, rp, graph, h_out, front.data(), front.size(), &n_out);
+  // the final x into the caller's buffer, the state record to the host
+  if (rc == CCM_OK) {
+    e = cudaStreamBeginCaptureToGraph(s, graph, &n_out, nullptr, 1, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      cg_final_x_kernel<<<grid_for(r.n), 256, 0, s>>>(r.d_ctl, r.xb[1], r.xb[0], r.n);
+      cudaMemcpyAsync(r.h_ctl, r.d_ctl, kCgCtlHead, cudaMemcpyDeviceToHost, s);
+      cudaStreamCaptureStatus cs;
+      const cudaGraphNode_t *deps = nullptr;
+      size_t nd = 0;
+      if (cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &nd) == cudaSuccess && nd == 1)
+        *last = deps[0];
+      else
+        e = cudaErrorUnknown;
+      cudaGraph_t tmp = nullptr;
+      const cudaError_t e2 = cudaStreamEndCapture(s, &tmp);
+      if (e == cudaSuccess) e = e2;
+    }
+    if (e != cudaSuccess) rc = set_last_error(CCM_ERR_CUDA, "ccm_solve_batch: %s", cudaGetErrorString(e));
+  }
+  c->prof_on = prof;
+  if (rc != CCM_OK) {
+    free_run(r);
+    delete gs;
+    return rc;
+  }
+  *out = gs;
+  return CCM_OK;
+}
+
+int ccm::cg_graph_solve_result(const CgGraphSolve *gs, ccm_cg_result *res) {
+  const CgCtl &h = *gs->r.h_ctl;
+  std::memset(res, 0, sizeof(*res));
+  res->status = h.status;
+  res->iterations = h.iter;
+  res->evaluations = h.evals;
+  res->fx = h.f;
+  res->gnorm = std::sqrt(h.gg);
+  if (h.status == CCM_ERR_DEVICE)
+    return set_last_error(CCM_ERR_DEVICE, "ccm_solve_batch: device wait timed out in an evaluation");
+  return CCM_OK;
+}
+
+void ccm::cg_graph_solve_free(CgGraphSolve *gs) {
+  if (!gs) return;
+  free_run(gs->r);
+  delete gs;
+}
 
 extern "C" {
 
@@ -453,7 +606,7 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
   rc = enqueue_evaluation(c, r.xb[0], r.gb[0]);
   if (rc == CCM_OK) {
     cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(r.gb[0], nullptr, nullptr, n, r.d_part);
-    cg_start_kernel<<<1, 256, 0, s>>>(r.d_ctl, r.d_part, kDotBlocks, c->d_out, nullptr);
+    cg_start_kernel<<<1, 256, 0, s>>>(r.d_ctl, r.d_part, kDotBlocks, c->d_out, nullptr, 0, 0);
     count_launch(c, 2);
     e = cudaMemcpyAsync(r.h_ctl, r.d_ctl, kCgCtlHead, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -539,7 +692,7 @@ int ccm::conjugrad_callback_gpu(float *d_x, long long n, ccm_eval_callback eval,
   if (e == cudaSuccess) e = evaluate(0);
   if (e == cudaSuccess) {
     cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(gb[0], nullptr, nullptr, n, d_part);
-    cg_start_kernel<<<1, 256, 0, s>>>(d_ctl, d_part, kDotBlocks, nullptr, d_f);
+    cg_start_kernel<<<1, 256, 0, s>>>(d_ctl, d_part, kDotBlocks, nullptr, d_f, 0, 0);
     e = cudaMemcpyAsync(h, d_ctl, kCgCtlHead, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   }

@@ -194,6 +194,19 @@ int conjugrad_host_vectors(float *x, long long n, ccm_eval_callback eval,
 // True when p points at a live context of this library.
 bool is_context(const void *p);
 
+// A whole device-side solve added to a graph that holds many (the batch
+// solver's waves): initial evaluation, the iteration loop, the final x in d_x,
+// the state record copied to pinned memory.  `last` receives the solve's last
+// node.  After the graph ran, cg_graph_solve_result reads the outcome.
+struct CgGraphSolve;
+int cg_graph_solve_add(ccm_context *c, float *d_x, const ccm_cg_params *params, cudaGraph_t graph,
+                       CgGraphSolve **out, cudaGraphNode_t *last);
+int cg_graph_solve_result(const CgGraphSolve *gs, ccm_cg_result *res);
+void cg_graph_solve_free(CgGraphSolve *gs);
+// Upper bound of the device memory of a context of `path` (bytes), without the
+// optimizer's vectors.
+size_t context_bytes_estimate(int L, int N, int path);
+
 constexpr uint32_t kContextMagic = 0xCC3B2000u;
 
 }  // namespace ccm

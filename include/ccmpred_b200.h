@@ -297,9 +297,12 @@ CCM_API int ccm_conjugrad_host(ccm_context *ctx, float *x, long long n,
 /* ---------------------------------------------------------------- batched solves */
 /* Many alignments of different sizes solved to convergence concurrently on
  * one GPU (no reference counterpart: the reference runs one alignment per
- * process).  Host worker threads each drive their own context and stream
- * through reweighting, init_bias, the device CG and the contact map;
- * alignments are taken largest-first. */
+ * process).  Alignments are taken largest-first.  Default (waves = 1): they are
+ * admitted in waves under a device-memory budget; the whole device-side solve
+ * of every alignment of a wave (initial evaluation, CG iterations in
+ * conditional graph nodes, contact scores) goes into ONE graph as independent
+ * branches, launched once per wave.  waves = 0: host worker threads each drive
+ * their own context and stream. */
 typedef struct ccm_msa_desc {
 	const unsigned char *msa;   /* nrow x ncol states 0..20, host memory */
 	int ncol;
@@ -317,6 +320,11 @@ typedef struct ccm_batch_params {
 	int sms_per_worker;          /* max_sms of every worker's contexts; 0 = no limit
 	                                (default; on B200 the 256-alignment batch ran
 	                                fastest with no limit) */
+	int waves;                   /* 1 (default): one graph launch per wave of
+	                                alignments; 0: host worker threads */
+	int wave_max;                /* most alignments in one wave (default 64) */
+	size_t wave_bytes;           /* device memory of one wave (estimated from the
+	                                alignments' sizes); 0 = 60 % of the free memory */
 	ccm_cg_params cg;            /* optimizer settings for every alignment */
 } ccm_batch_params;
 
@@ -326,7 +334,7 @@ typedef struct ccm_batch_result {
 	int evaluations;
 	int pad;
 	double fx;
-	double seconds;    /* wall time of this alignment's solve */
+	double seconds;    /* wall time of this alignment's solve (of its wave, with waves) */
 } ccm_batch_result;
 
 CCM_API void ccm_batch_params_default(ccm_batch_params *p);

@@ -11,15 +11,20 @@ pytestmark = pytest.mark.gpu
 
 
 def test_batch_matches_standalone_solves(gpu):
+    """The wave solver (all solves of a wave in one graph launch; several waves
+    here) and the host-thread solver (4 workers, and 1) give every alignment the
+    same result: the same kernels and rules run per alignment either way."""
     msas = synth.batch_workload(10, seed0=500)
     msas = [m[: min(len(m), 1500)] for m in msas]          # keep the test short
-    res4, maps4 = solve_batch(msas, workers=4, max_iterations=40)
-    res1, maps1 = solve_batch(msas, workers=1, max_iterations=40)
-    for r4, r1, m4, m1 in zip(res4, res1, maps4, maps1):
-        assert r4.status in (_lib.CG_SUCCESS, _lib.CG_ERR_MAXITER)
-        assert r4.iterations == r1.iterations and r4.fx == r1.fx
-        assert np.array_equal(m4, m1)
-        assert np.all(np.isfinite(m4))
+    resw, mapsw = solve_batch(msas, max_iterations=40, wave_max=4)
+    res4, maps4 = solve_batch(msas, workers=4, max_iterations=40, waves=False)
+    res1, maps1 = solve_batch(msas, workers=1, max_iterations=40, waves=False)
+    for rw, r4, r1, mw, m4, m1 in zip(resw, res4, res1, mapsw, maps4, maps1):
+        assert rw.status in (_lib.CG_SUCCESS, _lib.CG_ERR_MAXITER)
+        assert rw.iterations == r4.iterations == r1.iterations
+        assert rw.evaluations == r4.evaluations and rw.fx == r4.fx == r1.fx
+        assert np.array_equal(mw, m4) and np.array_equal(m4, m1)
+        assert np.all(np.isfinite(mw))
 
 
 @pytest.mark.parametrize("gradient", ["tied", "partial"])
@@ -45,8 +50,8 @@ def test_sm_share_gives_identical_results(gpu, gradient):
 
 def test_batch_with_explicit_share(gpu):
     msas = [m[:800] for m in synth.batch_workload(4, seed0=600)]
-    ra, ma = solve_batch(msas, workers=2, max_iterations=15, sms_per_worker=12)
-    rb, mb = solve_batch(msas, workers=2, max_iterations=15, sms_per_worker=-1)
+    ra, ma = solve_batch(msas, workers=2, max_iterations=15, sms_per_worker=12, waves=False)
+    rb, mb = solve_batch(msas, workers=2, max_iterations=15, sms_per_worker=-1, waves=False)
     for a, b, x, y in zip(ra, rb, ma, mb):
         assert a.iterations == b.iterations and a.fx == b.fx
         assert np.array_equal(x, y)
