@@ -348,16 +348,30 @@ def run_batch(args, world, rank, local):
     import ccmpred_b200 as cb
     from ccmpred_b200 import synth
     torch.cuda.set_device(local)
+    from ccmpred_b200 import autotune
     msas = synth.batch_workload(256, seed0=1000 + 1000 * rank)
     cb.solve_batch(msas[:2], workers=2, max_iterations=3, epsilon=1e-3, device=local)  # warm-up
     torch.cuda.synchronize()
-    barrier(world)
-    t0 = time.perf_counter()
-    res, _ = cb.solve_batch(msas, workers=args.batch_workers, path=args.path, max_iterations=250,
-                            epsilon=1e-3,
-                            device=local)
-    torch.cuda.synchronize()
-    el = max_over_ranks(world, time.perf_counter() - t0)
+    # the headline: waves (one graph launch per wave), each alignment's path from the
+    # autotuner's table when it exists; beside it the same with one path for all and
+    # with host worker threads
+    runs = [("waves", "auto" if autotune.load() else args.path), ("waves", args.path),
+            ("threads", args.path)]
+    if runs[0] == runs[1]:
+        runs = runs[1:]
+    timed = {}
+    res = None
+    for mode, path in runs:
+        barrier(world)
+        t0 = time.perf_counter()
+        r, _ = cb.solve_batch(msas, workers=args.batch_workers, path=path, max_iterations=250,
+                              epsilon=1e-3, device=local, waves=(mode == "waves"))
+        torch.cuda.synchronize()
+        el_r = max_over_ranks(world, time.perf_counter() - t0)
+        timed[f"{mode}/{path}"] = {"msas_per_s": world * len(msas) / el_r, "wall_s": el_r,
+                                   "iterations_mean": float(np.mean([x.iterations for x in r]))}
+        if res is None:
+            res, el = r, el_r
     value = world * len(msas) / el
     if rank != 0:
         return
@@ -380,8 +394,9 @@ def run_batch(args, world, rank, local):
         "data": "synthetic", "dtype": "int8",
         "config": {"workload": "batch256: L~U[50,400], N~logU[200,20000], seeds 1000+i, "
                                "eps 1e-3 or 250 iterations",
-                   "workers": args.batch_workers, "path": args.path},
+                   "mode": f"{runs[0][0]}/{runs[0][1]}"},
         "wall_s": el, "solved_ok": ok, "iterations_mean": float(its.mean()),
+        "by_mode": timed,
         "plain_f32_one_at_a_time": {
             "msas_per_s_extrapolated": len(msas) / plain_total,
             "sample": f"{k} alignments stratified by N*L^2, timed one at a time, "

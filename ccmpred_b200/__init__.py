@@ -62,19 +62,31 @@ def solve_batch(msas, workers: int = 8, path: str = "tc_i8sp", threshold: float 
                 wave_max: int = 64, wave_bytes: int = 0):
     """Solve many alignments to convergence concurrently (ccm_solve_batch).
 
+    ``path="auto"`` takes each alignment's path from the table that
+    ``ccmpred_b200.autotune`` measured on the GPU.
     ``waves`` (default): one graph launch per wave of alignments (``wave_max``
     alignments at most, ``wave_bytes`` of device memory, 0 = 60 % of the free
     memory); else ``workers`` host threads with a context and stream each.
     Returns (results, maps): per-alignment CcmBatchResult and APC contact maps."""
     arrs = [np.ascontiguousarray(m, dtype=np.uint8) for m in msas]
     n = len(arrs)
+    table = None
+    if path == "auto":
+        # the per-size choice of ccmpred_b200.autotune (tuning_b200.json)
+        from . import autotune
+        table = autotune.load()
+        if table is None:
+            raise FileNotFoundError("path='auto' needs the table of ccmpred_b200.autotune "
+                                    f"({autotune.TABLE}); run `python -m ccmpred_b200.autotune`")
     descs = (_lib.CcmMsaDesc * max(n, 1))()
     for i, a in enumerate(arrs):
         descs[i].msa = a.ctypes.data
         descs[i].nrow, descs[i].ncol = a.shape
+        descs[i].path = PATHS[autotune.choose(table, a.shape[1], a.shape[0])] if table else -1
     p = _lib.CcmBatchParams()
     lib().ccm_batch_params_default(ctypes.byref(p))
-    p.workers, p.path, p.reweighting_threshold, p.device = workers, PATHS[path], threshold, device
+    p.workers, p.reweighting_threshold, p.device = workers, threshold, device
+    p.path = PATHS["tc_i8sp" if path == "auto" else path]
     p.sms_per_worker = sms_per_worker
     p.waves, p.wave_max, p.wave_bytes = int(bool(waves)), wave_max, wave_bytes
     p.cg.max_iterations, p.cg.epsilon = max_iterations, epsilon

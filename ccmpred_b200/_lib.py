@@ -78,7 +78,8 @@ CG_ERR_LINESEARCH = -1022
 CG_ERR_NONFINITE = -1021
 
 class CcmMsaDesc(ctypes.Structure):
-    _fields_ = [("msa", ctypes.c_void_p), ("ncol", ctypes.c_int), ("nrow", ctypes.c_int)]
+    _fields_ = [("msa", ctypes.c_void_p), ("ncol", ctypes.c_int), ("nrow", ctypes.c_int),
+                ("path", ctypes.c_int), ("pad", ctypes.c_int)]
 
 
 class CcmBatchParams(ctypes.Structure):

@@ -102,7 +102,7 @@ int solve_waves(int n, const ccm_msa_desc *msas, const ccm_batch_params *params,
     size_t bytes = 0;
     while (pos < order.size() && (int)wave.size() < wave_max) {
       const ccm_msa_desc &m = msas[order[pos]];
-      const size_t need = context_bytes_estimate(m.ncol, m.nrow, params->path) +
+      const size_t need = context_bytes_estimate(m.ncol, m.nrow, m.path >= 0 ? m.path : params->path) +
                           5 * sizeof(float) * (size_t)ccm_nvar_padded(m.ncol) +
                           sizeof(float) * (size_t)m.ncol * m.ncol;
       if (!wave.empty() && bytes + need > budget) break;
@@ -133,7 +133,7 @@ int solve_waves(int n, const ccm_msa_desc *msas, const ccm_batch_params *params,
         ccm_options_default(&o, L);
         o.lambda_single = params->lambda_single;
         o.lambda_pair = params->lambda_pair_factor * (float)(L - 1);
-        o.path = params->path;
+        o.path = m.path >= 0 ? m.path : params->path;
         o.device = dev;
         o.stream = stream;
         rc = create_context(&it.ctx, m.msa, L, N, w.data(), &o, pool);
@@ -237,7 +237,9 @@ int ccm_solve_batch(int n, const ccm_msa_desc *msas, const ccm_batch_params *par
                     ccm_batch_result *results, float **contact_maps) {
   if (n < 0 || (n > 0 && (!msas || !results)) || !params || params->workers < 1) return CCM_ERR_INVALID;
   for (int i = 0; i < n; ++i)
-    if (!msas[i].msa || msas[i].ncol <= 0 || msas[i].nrow <= 0) return CCM_ERR_INVALID;
+    if (!msas[i].msa || msas[i].ncol <= 0 || msas[i].nrow <= 0 || msas[i].path > CCM_PATH_TC_I8SP ||
+        msas[i].path == CCM_PATH_SIMT_F64)
+      return CCM_ERR_INVALID;
   std::vector<int> order(n);
   std::iota(order.begin(), order.end(), 0);
   std::sort(order.begin(), order.end(), [&](int a, int b) {
@@ -311,7 +313,7 @@ int ccm_solve_batch(int n, const ccm_msa_desc *msas, const ccm_batch_params *par
         ccm_options_default(&o, L);
         o.lambda_single = params->lambda_single;
         o.lambda_pair = params->lambda_pair_factor * (float)(L - 1);
-        o.path = params->path;
+        o.path = m.path >= 0 ? m.path : params->path;
         o.device = params->device;
         o.stream = stream;
         o.max_sms = max_sms;

@@ -307,6 +307,9 @@ typedef struct ccm_msa_desc {
 	const unsigned char *msa;   /* nrow x ncol states 0..20, host memory */
 	int ncol;
 	int nrow;
+	int path;                   /* CCM_PATH_* for this alignment, or -1: the batch's
+	                               path (ccmpred_b200.autotune picks one per size) */
+	int pad;
 } ccm_msa_desc;
 
 typedef struct ccm_batch_params {

@@ -80,3 +80,17 @@ def test_errors_are_reported_without_gpu():
                         3, 4, None, None)
     assert rc == _lib.CCM_ERR_INVALID
     assert b"state" in lib.ccm_last_error()
+
+
+def test_batch_descriptor_layout_and_autotune_choice():
+    from ccmpred_b200 import _lib, autotune
+    assert ctypes.sizeof(_lib.CcmMsaDesc) == 24 and _lib.CcmMsaDesc.path.offset == 16
+    table = {"buckets_L": [60, 200], "buckets_N": [300, 3000],
+             "rows": [{"L": 60, "N": 300, "path": "simt_f32"},
+                      {"L": 60, "N": 3000, "path": "tc_bf16x2"},
+                      {"L": 200, "N": 300, "path": "tc_i8x3"},
+                      {"L": 200, "N": 3000, "path": "tc_i8sp"}]}
+    assert autotune.choose(table, 50, 250) == "simt_f32"
+    assert autotune.choose(table, 60, 301) == "tc_bf16x2"
+    assert autotune.choose(table, 61, 100) == "tc_i8x3"
+    assert autotune.choose(table, 900, 90000) == "tc_i8sp"   # beyond the table: largest bucket
