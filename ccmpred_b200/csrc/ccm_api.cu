@@ -25,6 +25,22 @@ void prof_mark(ccm_context *c) {
 
 void count_launch(ccm_context *c, int n) { c->launches += n; }
 
+// Zero `words` 32-bit words.  A kernel rather than cudaMemsetAsync: the
+// evaluation is also captured into the bodies of conditional graph nodes (the
+// device-side CG), which hold kernel nodes.
+__global__ void zero_words_kernel(uint32_t *__restrict__ p, long long words) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < words;
+       i += (long long)gridDim.x * blockDim.x)
+    p[i] = 0u;
+}
+
+cudaError_t zero_words(void *p, long long words, cudaStream_t s) {
+  const long long blocks = (words + 255) / 256;
+  zero_words_kernel<<<(unsigned)(blocks < 1184 ? (blocks > 0 ? blocks : 1) : 1184), 256, 0, s>>>(
+      static_cast<uint32_t *>(p), words);
+  return cudaGetLastError();
+}
+
 bool is_context(const void *p) {
   return p && static_cast<const ccm_context *>(p)->magic == kContextMagic;
 }
@@ -366,7 +382,8 @@ int check_status(ccm_context *c) {
 }
 
 int enqueue_eval(ccm_context *c, const float *d_x, float *d_g) {
-  CCM_CUDA_TRY(cudaMemsetAsync(c->d_out, 0, sizeof(ccm_result), c->stream));
+  CCM_CUDA_TRY(zero_words(c->d_out, sizeof(ccm_result) / 4, c->stream));
+  count_launch(c);
   c->prof_idx = 0;
   cudaError_t e;
   switch (c->path) {
@@ -405,7 +422,8 @@ int ccm::enqueue_evaluation_step(ccm_context *c, const float *d_x, const float *
   const bool i8 = c->path == CCM_PATH_TC_I8X3 || c->path == CCM_PATH_TC_I8SP;
   if (c->path != CCM_PATH_TC_BF16X2 && c->path != CCM_PATH_TC_BF16X3 && !i8)
     return set_error(CCM_ERR_INVALID, "fused step: tensor-core paths only");
-  CCM_CUDA_TRY(cudaMemsetAsync(c->d_out, 0, sizeof(ccm_result), c->stream));
+  CCM_CUDA_TRY(zero_words(c->d_out, sizeof(ccm_result) / 4, c->stream));
+  count_launch(c);
   c->prof_idx = 0;
   const cudaError_t e = i8
                             ? i8_evaluate(c, d_x, d_g, d_s, d_alpha, d_xt)

@@ -126,12 +126,17 @@ __device__ double reduce_part(const double *part, int nblocks, int k, double *re
 
 // Conditional-node values a control kernel sets.  mode 0: none (host-driven);
 // 1: the line search's WHILE only (one graph per iteration); 2: the whole solve
-// (line searches of both parities, the IF that runs the parity-1 iteration, the
-// outer WHILE).
+// (its line search's WHILE, the IF that runs the parity-1 iteration, the outer
+// WHILE).  A kernel sets only the values of conditional nodes that enclose it
+// (their handles belong to its graph or to a graph around it); each inner WHILE
+// is re-opened by an arm kernel in the graph that holds it.
 struct CgHandles {
-  cudaGraphConditionalHandle ls_self, ls_other, it2, outer;
+  cudaGraphConditionalHandle ls_self, it2, outer;
   int mode, parity;
 };
+
+// Opens a WHILE node for its next execution: value 1.
+__global__ void cg_arm_kernel(cudaGraphConditionalHandle h) { cudaGraphSetConditional(h, 1u); }
 
 // After the initial evaluation: f0 (from the evaluation record, or from f_slot
 // when a callback evaluated), g0.g0 from the partials.  In a graph (set_out) it
@@ -190,7 +195,6 @@ __global__ void __launch_bounds__(256) cg_control_kernel(CgCtl *ctl, CgRuleParam
   if (h.mode == 2 && (accepted || !running)) {
     cudaGraphSetConditional(h.outer, running ? 1u : 0u);
     if (h.parity == 0) cudaGraphSetConditional(h.it2, running ? 1u : 0u);
-    cudaGraphSetConditional(h.ls_other, running ? 1u : 0u);
   }
 }
 
@@ -288,8 +292,10 @@ int enqueue_trial(CgRun &r, int p, const CgRuleParams &rp, CgHandles h) {
 cudaError_t add_conditional(cudaGraph_t graph, cudaGraphConditionalNodeType type, unsigned deflt,
                             const cudaGraphNode_t *deps, size_t ndeps,
                             cudaGraphConditionalHandle *handle, cudaGraphNode_t *node,
-                            cudaGraph_t *body) {
-  cudaError_t e = cudaGraphConditionalHandleCreate(handle, graph, deflt, cudaGraphCondAssignDefault);
+                            cudaGraph_t *body, bool have_handle = false) {
+  cudaError_t e = have_handle ? cudaSuccess
+                              : cudaGraphConditionalHandleCreate(handle, graph, deflt,
+                                                                 cudaGraphCondAssignDefault);
   if (e != cudaSuccess) return e;
   cudaGraphNodeParams np = {};
   np.type = cudaGraphNodeTypeConditional;
@@ -331,15 +337,38 @@ int capture_readback(CgRun &r, cudaGraph_t graph, cudaGraphNode_t dep) {
   return CCM_OK;
 }
 
+// An arm kernel for handle h as the first node of `graph` (captured through the
+// context's stream); its node in *node.
+int capture_arm(CgRun &r, cudaGraph_t graph, cudaGraphConditionalHandle h, cudaGraphNode_t *node) {
+  cudaStream_t s = r.c->stream;
+  cudaError_t e = cudaStreamBeginCaptureToGraph(s, graph, nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cg_arm_kernel<<<1, 1, 0, s>>>(h);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    e = cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &nd);
+    if (e == cudaSuccess && nd == 1) *node = deps[0];
+    else if (e == cudaSuccess) e = cudaErrorUnknown;
+    cudaGraph_t tmp = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(s, &tmp);
+    if (e == cudaSuccess) e = e2;
+  }
+  if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "cg capture: %s", cudaGetErrorString(e));
+  return CCM_OK;
+}
+
 // The iteration loop of a whole solve, added to `g` after `deps`:
-// WHILE(outer) { WHILE(ls0) { trial parity 0 }; IF(it2) { WHILE(ls1) { trial
-// parity 1 } } }.  The outer WHILE node's handle h_out exists already (a kernel
-// before the loop may set it).
+//   WHILE(outer) { arm(ls0); WHILE(ls0) { trial parity 0 };
+//                  IF(it2) { arm(ls1); WHILE(ls1) { trial parity 1 } } }
+// The outer WHILE node's handle h_out exists already (a kernel before the loop
+// may set it).
 int add_solve_loop(CgRun &r, const CgRuleParams &rp, cudaGraph_t g,
                    cudaGraphConditionalHandle h_out, const cudaGraphNode_t *deps, size_t ndeps,
                    cudaGraphNode_t *n_out) {
   cudaGraphConditionalHandle h_ls0, h_it2, h_ls1;
-  cudaGraphNode_t n_ls0, n_it2, n_ls1;
+  cudaGraphNode_t n_ls0, n_it2, n_ls1, n_arm0, n_arm1;
   cudaGraph_t b_out = nullptr, b_ls0, b_it2, b_ls1;
   cudaGraphNodeParams np = {};
   np.type = cudaGraphNodeTypeConditional;
@@ -349,15 +378,25 @@ int add_solve_loop(CgRun &r, const CgRuleParams &rp, cudaGraph_t g,
   cudaError_t e = cudaGraphAddNode(n_out, g, deps, ndeps, &np);
   if (e == cudaSuccess) b_out = np.conditional.phGraph_out[0];
   if (e == cudaSuccess)
-    e = add_conditional(b_out, cudaGraphCondTypeWhile, 1, nullptr, 0, &h_ls0, &n_ls0, &b_ls0);
-  if (e == cudaSuccess)
-    e = add_conditional(b_out, cudaGraphCondTypeIf, 0, &n_ls0, 1, &h_it2, &n_it2, &b_it2);
-  if (e == cudaSuccess)
-    e = add_conditional(b_it2, cudaGraphCondTypeWhile, 1, nullptr, 0, &h_ls1, &n_ls1, &b_ls1);
-  int rc = CCM_OK;
-  if (e != cudaSuccess) rc = set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
-  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls0, 0, rp, CgHandles{h_ls0, h_ls1, h_it2, h_out, 2, 0});
-  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls1, 1, rp, CgHandles{h_ls1, h_ls0, h_it2, h_out, 2, 1});
+    e = cudaGraphConditionalHandleCreate(&h_ls0, b_out, 1, cudaGraphCondAssignDefault);
+  int rc = e == cudaSuccess ? CCM_OK
+                            : set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
+  if (rc == CCM_OK) rc = capture_arm(r, b_out, h_ls0, &n_arm0);
+  if (rc == CCM_OK) {
+    e = add_conditional(b_out, cudaGraphCondTypeWhile, 1, &n_arm0, 1, &h_ls0, &n_ls0, &b_ls0, true);
+    if (e == cudaSuccess)
+      e = add_conditional(b_out, cudaGraphCondTypeIf, 0, &n_ls0, 1, &h_it2, &n_it2, &b_it2);
+    if (e == cudaSuccess)
+      e = cudaGraphConditionalHandleCreate(&h_ls1, b_it2, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) rc = set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
+  }
+  if (rc == CCM_OK) rc = capture_arm(r, b_it2, h_ls1, &n_arm1);
+  if (rc == CCM_OK) {
+    e = add_conditional(b_it2, cudaGraphCondTypeWhile, 1, &n_arm1, 1, &h_ls1, &n_ls1, &b_ls1, true);
+    if (e != cudaSuccess) rc = set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
+  }
+  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls0, 0, rp, CgHandles{h_ls0, h_it2, h_out, 2, 0});
+  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls1, 1, rp, CgHandles{h_ls1, h_it2, h_out, 2, 1});
   return rc;
 }
 
@@ -393,7 +432,7 @@ int build_iteration_graph(CgRun &r, int p, const CgRuleParams &rp) {
   e = add_conditional(g, cudaGraphCondTypeWhile, 1, nullptr, 0, &h_ls, &n_ls, &b_ls);
   int rc = e == cudaSuccess ? CCM_OK
                             : set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
-  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls, p, rp, CgHandles{h_ls, h_ls, h_ls, h_ls, 1, p});
+  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls, p, rp, CgHandles{h_ls, h_ls, h_ls, 1, p});
   if (rc == CCM_OK) rc = capture_readback(r, g, n_ls);
   if (rc == CCM_OK) {
     e = cudaGraphInstantiate(&r.exec[1 + p], g, 0);
@@ -680,7 +719,7 @@ int ccm::conjugrad_callback_gpu(float *d_x, long long n, ccm_eval_callback eval,
   CgCtl *h = static_cast<CgCtl *>(pinned_small_alloc(kCgCtlHead));
   double *h_f = static_cast<double *>(pinned_small_alloc(sizeof(double)));
   if (e == cudaSuccess && (!h || !h_f)) e = cudaErrorMemoryAllocation;
-  const CgHandles none{0, 0, 0, 0, 0, 0};
+  const CgHandles none{0, 0, 0, 0, 0};
   int stopped = 0;
   // one evaluation by the callback at xb[q] into gb[q]; its f goes to the device
   auto evaluate = [&](int q) -> cudaError_t {

@@ -142,6 +142,9 @@ cudaError_t launch_contact_scores(const float *d_x, float *d_out, int L, cudaStr
 void *pinned_small_alloc(size_t bytes);
 void pinned_small_free(void *p);
 void count_launch(ccm_context *c, int n = 1);
+// Zero `words` 32-bit words on stream s with a kernel (capturable into the
+// bodies of conditional graph nodes).
+cudaError_t zero_words(void *p, long long words, cudaStream_t s);
 
 cudaError_t tc_configure_kernels();
 // CTA pairs of tc_forward that can be resident at once on the current device.

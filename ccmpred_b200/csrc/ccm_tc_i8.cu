@@ -1327,8 +1327,7 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   cudaError_t e;
 
   prof_mark(c);
-  if ((e = cudaMemsetAsync(c->d_colmax, 0, sizeof(uint32_t) * kQ * L, c->stream)) != cudaSuccess)
-    return e;
+  if ((e = zero_words(c->d_colmax, (long long)kQ * L, c->stream)) != cudaSuccess) return e;
   constexpr int kRows = 32;
   const dim3 cgrid((kQPad * L + 255) / 256, (kQ * L + kRows - 1) / kRows + (step ? 1 : 0));
   if (step)
@@ -1403,7 +1402,7 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
 
   launch_tc_finalize(c, x1, d_g, 2LL * pair_tiles);
   prof_mark(c);
-  count_launch(c, 6);
+  count_launch(c, 7);
   return cudaGetLastError();
 }
 
