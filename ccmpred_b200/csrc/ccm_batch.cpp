@@ -170,8 +170,9 @@ int solve_waves(int n, const ccm_msa_desc *msas, const ccm_batch_params *params,
     }
     if (rc == CCM_OK) {
       e = cudaStreamSynchronize(stream);  // contexts and x set up before the launch
-      if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-      if (e == cudaSuccess) e = cudaGraphLaunch(exec, stream);
+      if (e == cudaSuccess && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+        rc = set_last_error(CCM_ERR_UNSUPPORTED, "ccm_solve_batch: the wave's graph");
+      if (e == cudaSuccess && rc == CCM_OK) e = cudaGraphLaunch(exec, stream);
       if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
       if (e != cudaSuccess) rc = set_last_error(CCM_ERR_CUDA, "ccm_solve_batch: %s", cudaGetErrorString(e));
     }
@@ -247,7 +248,12 @@ int ccm_solve_batch(int n, const ccm_msa_desc *msas, const ccm_batch_params *par
     const double cb = (double)msas[b].nrow * msas[b].ncol * msas[b].ncol;
     return ca > cb;
   });
-  if (params->waves) return solve_waves(n, msas, params, results, contact_maps, order);
+  if (params->waves) {
+    const int rc = solve_waves(n, msas, params, results, contact_maps, order);
+    if (rc != CCM_ERR_UNSUPPORTED) return rc;
+    // nested conditional nodes refused by this driver: host worker threads
+    (void)cudaGetLastError();
+  }
   const int nw = std::min(params->workers, std::max(n, 1));
   // An optional share of the SMs for each worker's contexts.  Measured on B200,
   // no share is faster: the prep and CG kernels spread over every SM anyway,

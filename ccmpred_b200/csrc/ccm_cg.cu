@@ -24,7 +24,7 @@
 // line-search quantity is FP64.
 //
 // conjugrad_gpu with another evaluate callback than this library's own
-// (ccm_conjugrad_callback_gpu below) runs the same kernels around one call of
+// (conjugrad_callback_gpu below) runs the same kernels around one call of
 // the callback per trial, from the host.
 #include <cmath>
 #include <cstdio>
@@ -135,8 +135,31 @@ struct CgHandles {
   int mode, parity;
 };
 
-// Opens a WHILE node for its next execution: value 1.
-__global__ void cg_arm_kernel(cudaGraphConditionalHandle h) { cudaGraphSetConditional(h, 1u); }
+// Opens a WHILE node for its next execution while the solve runs.
+__global__ void cg_arm_kernel(const CgCtl *ctl, cudaGraphConditionalHandle h) {
+  cudaGraphSetConditional(h, ctl->status == kCgRunning ? 1u : 0u);
+}
+
+// First node of every round of the whole-solve graph's outer loop: counts the
+// round and opens the first line search while the solve runs.  It bounds the
+// loop on its own: past max_rounds (two iterations per round, so a solve within
+// max_iterations never gets there) it ends the solve with CCM_ERR_DEVICE and
+// closes the outer loop, whatever the other nodes did.
+__global__ void cg_guard_kernel(CgCtl *ctl, cudaGraphConditionalHandle h_out,
+                                cudaGraphConditionalHandle h_ls0, cudaGraphConditionalHandle h_it2,
+                                int max_rounds) {
+  const int round = ++ctl->rounds;
+  if (ctl->status == kCgRunning && round > max_rounds) {
+    ctl->status = CCM_ERR_DEVICE;
+    ctl->ls_active = 0;
+  }
+  const bool go = ctl->status == kCgRunning;
+  cudaGraphSetConditional(h_ls0, go ? 1u : 0u);
+  if (!go) {
+    cudaGraphSetConditional(h_it2, 0u);
+    cudaGraphSetConditional(h_out, 0u);
+  }
+}
 
 // After the initial evaluation: f0 (from the evaluation record, or from f_slot
 // when a callback evaluated), g0.g0 from the partials.  In a graph (set_out) it
@@ -180,6 +203,10 @@ __global__ void __launch_bounds__(256) cg_control_kernel(CgCtl *ctl, CgRuleParam
   t.gtg = reduce_part(part, nblocks, 2, red);
   t.xtxt = with_xx ? reduce_part(part + 3 * nblocks, nblocks, 1, red) : 0.0;
   if (threadIdx.x != 0) return;
+  if (ctl->status != kCgRunning) {  // a finished solve takes no more trials
+    if (h.mode >= 1) cudaGraphSetConditional(h.ls_self, 0u);
+    return;
+  }
   t.f = f_slot ? *f_slot : res->fx;
   t.status = res ? res->status : 0;
   t.pad = 0;
@@ -337,14 +364,18 @@ int capture_readback(CgRun &r, cudaGraph_t graph, cudaGraphNode_t dep) {
   return CCM_OK;
 }
 
-// An arm kernel for handle h as the first node of `graph` (captured through the
-// context's stream); its node in *node.
-int capture_arm(CgRun &r, cudaGraph_t graph, cudaGraphConditionalHandle h, cudaGraphNode_t *node) {
+// The first node of `graph` (captured through the context's stream): an arm
+// kernel for handle h, or, with h_out, the guard of the outer loop; its node in
+// *node.
+int capture_arm(CgRun &r, cudaGraph_t graph, cudaGraphConditionalHandle h, cudaGraphNode_t *node,
+                const cudaGraphConditionalHandle *h_out = nullptr,
+                const cudaGraphConditionalHandle *h_it2 = nullptr, int max_rounds = 0) {
   cudaStream_t s = r.c->stream;
   cudaError_t e = cudaStreamBeginCaptureToGraph(s, graph, nullptr, nullptr, 0,
                                                 cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    cg_arm_kernel<<<1, 1, 0, s>>>(h);
+    if (h_out) cg_guard_kernel<<<1, 1, 0, s>>>(r.d_ctl, *h_out, h, *h_it2, max_rounds);
+    else cg_arm_kernel<<<1, 1, 0, s>>>(r.d_ctl, h);
     cudaStreamCaptureStatus cs;
     const cudaGraphNode_t *deps = nullptr;
     size_t nd = 0;
@@ -360,10 +391,11 @@ int capture_arm(CgRun &r, cudaGraph_t graph, cudaGraphConditionalHandle h, cudaG
 }
 
 // The iteration loop of a whole solve, added to `g` after `deps`:
-//   WHILE(outer) { arm(ls0); WHILE(ls0) { trial parity 0 };
+//   WHILE(outer) { guard(ls0); WHILE(ls0) { trial parity 0 };
 //                  IF(it2) { arm(ls1); WHILE(ls1) { trial parity 1 } } }
 // The outer WHILE node's handle h_out exists already (a kernel before the loop
-// may set it).
+// may set it).  The guard bounds the rounds by itself, so the loop ends even if
+// the line searches' nodes did not.
 int add_solve_loop(CgRun &r, const CgRuleParams &rp, cudaGraph_t g,
                    cudaGraphConditionalHandle h_out, const cudaGraphNode_t *deps, size_t ndeps,
                    cudaGraphNode_t *n_out) {
@@ -379,13 +411,15 @@ int add_solve_loop(CgRun &r, const CgRuleParams &rp, cudaGraph_t g,
   if (e == cudaSuccess) b_out = np.conditional.phGraph_out[0];
   if (e == cudaSuccess)
     e = cudaGraphConditionalHandleCreate(&h_ls0, b_out, 1, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess)
+    e = cudaGraphConditionalHandleCreate(&h_it2, b_out, 0, cudaGraphCondAssignDefault);
   int rc = e == cudaSuccess ? CCM_OK
                             : set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
-  if (rc == CCM_OK) rc = capture_arm(r, b_out, h_ls0, &n_arm0);
+  if (rc == CCM_OK) rc = capture_arm(r, b_out, h_ls0, &n_arm0, &h_out, &h_it2, rp.max_iterations + 2);
   if (rc == CCM_OK) {
     e = add_conditional(b_out, cudaGraphCondTypeWhile, 1, &n_arm0, 1, &h_ls0, &n_ls0, &b_ls0, true);
     if (e == cudaSuccess)
-      e = add_conditional(b_out, cudaGraphCondTypeIf, 0, &n_ls0, 1, &h_it2, &n_it2, &b_it2);
+      e = add_conditional(b_out, cudaGraphCondTypeIf, 0, &n_ls0, 1, &h_it2, &n_it2, &b_it2, true);
     if (e == cudaSuccess)
       e = cudaGraphConditionalHandleCreate(&h_ls1, b_it2, 1, cudaGraphCondAssignDefault);
     if (e != cudaSuccess) rc = set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
@@ -461,7 +495,9 @@ int finish(CgRun &r, float *d_x, ccm_cg_result *result, int stopped) {
   const int dev_err = h.status == CCM_ERR_DEVICE;
   free_run(r);
   if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "ccm_conjugrad_gpu: %s", cudaGetErrorString(e));
-  if (dev_err) return set_last_error(CCM_ERR_DEVICE, "ccm_conjugrad_gpu: device wait timed out in an evaluation");
+  if (dev_err)
+    return set_last_error(CCM_ERR_DEVICE, "ccm_conjugrad_gpu: a device-side wait or loop bound "
+                                          "was reached (timed out in an evaluation)");
   if (result) *result = res;
   return CCM_OK;
 }
@@ -652,10 +688,18 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
     if (e != cudaSuccess) rc = set_last_error(CCM_ERR_CUDA, "ccm_conjugrad_gpu: %s", cudaGetErrorString(e));
   }
   // the graphs: the whole solve without a progress callback, else one per parity
+  bool whole = progress == nullptr;
   if (rc == CCM_OK && r.h_ctl->status == kCgRunning) {
     if (!progress) {
       rc = build_solve_graph(r, rp);
-    } else {
+      if (rc == CCM_ERR_UNSUPPORTED) {
+        // nested conditional nodes refused by this driver: one graph per iteration
+        (void)cudaGetLastError();
+        whole = false;
+        rc = CCM_OK;
+      }
+    }
+    if (rc == CCM_OK && !whole) {
       rc = build_iteration_graph(r, 0, rp);
       if (rc == CCM_OK) rc = build_iteration_graph(r, 1, rp);
     }
@@ -665,7 +709,7 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
 
   int stopped = 0;
   if (r.h_ctl->status == kCgRunning) {
-    if (!progress) {
+    if (whole) {
       e = cudaGraphLaunch(r.exec[0], s);
       if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     } else {
@@ -675,7 +719,7 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) break;
         const CgCtl &h = *r.h_ctl;
-        if (h.iter > iter0 &&
+        if (h.iter > iter0 && progress &&
             progress(instance, r.xb[h.parity], r.gb[h.parity], (float)h.f, (float)std::sqrt(h.xx),
                      (float)std::sqrt(h.gg), (float)h.step, (int)n, h.iter, h.ls_last)) {
           stopped = 1;

@@ -73,7 +73,8 @@ struct CgCtl {
   int parity;           // x is buffer `parity` (the trial writes the other one)
   int status;           // kCgRunning, or the CCM_CG_* outcome (CCM_ERR_DEVICE: a kernel timed out)
   int ls_active;        // 1 while the current line search continues
-  int pad[2];
+  int rounds;           // rounds of the whole-solve graph's outer loop (its bound)
+  int pad;
   double fhist[kCgHist];  // f after iteration i at i % kCgHist
 };
 constexpr int kCgCtlHead = 8 * 8 + 12 * 4;  // bytes before fhist
@@ -95,6 +96,7 @@ __host__ __device__ inline void cg_rules_start(CgCtl &c, double f0, double gg0) 
   c.beta = 0.0;
   c.step = 0.0;
   c.parity = 0;
+  c.rounds = 0;
   if (!cg_finite(f0)) {
     c.status = CCM_CG_ERR_NONFINITE;
   } else if (!(gg0 > 0.0)) {
