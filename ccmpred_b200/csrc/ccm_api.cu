@@ -46,8 +46,12 @@ bool is_context(const void *p) {
 }
 
 cudaError_t dev_alloc_raw(ccm_context *c, void **p, size_t bytes) {
-  return c->pool ? cudaMallocFromPoolAsync(p, bytes, c->pool, c->stream)
-                 : cudaMallocAsync(p, bytes, c->stream);
+  // the cap of ccm_options.mem_limit: the bytes this context holds
+  if (c->mem_limit > 0 && c->mem_used + bytes > c->mem_limit) return cudaErrorMemoryAllocation;
+  const cudaError_t e = c->pool ? cudaMallocFromPoolAsync(p, bytes, c->pool, c->stream)
+                                : cudaMallocAsync(p, bytes, c->stream);
+  if (e == cudaSuccess) c->mem_used += bytes;
+  return e;
 }
 
 // Small pinned host records (a context's result, the CG's step scalars) come
@@ -369,8 +373,6 @@ void free_all(ccm_context *c) {
     std::free(c->prof_events);
   }
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
-  // released by CUDA once the stream-ordered frees above have run
-  if (c->own_pool && c->pool) cudaMemPoolDestroy(c->pool);
 }
 
 int check_status(ccm_context *c) {
@@ -533,25 +535,9 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
   int rc = ensure_configured(o.device);
   if (rc != CCM_OK) return rc;
 
-  bool own_pool = false;
-  if (o.mem_limit > 0 && !pool) {
-    // a private pool whose maximum size is the cap (rounded up to 2 MiB)
-    cudaMemPoolProps props;
-    std::memset(&props, 0, sizeof(props));
-    props.allocType = cudaMemAllocationTypePinned;
-    props.handleTypes = cudaMemHandleTypeNone;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = o.device;
-    props.maxSize = (o.mem_limit + (2u << 20) - 1) & ~(size_t)((2u << 20) - 1);
-    cudaError_t e = cudaMemPoolCreate(&pool, &props);
-    if (e != cudaSuccess)
-      return set_error(CCM_ERR_CUDA, "ccm_create: memory pool of %zu bytes: %s", props.maxSize,
-                       cudaGetErrorString(e));
-    own_pool = true;
-  }
   ccm_context *c = new ccm_context();
   c->pool = pool;
-  c->own_pool = own_pool;
+  c->mem_limit = o.mem_limit;
   c->r_exp = r_exp;
   c->device = o.device;
   c->num_sms = prop.multiProcessorCount;
@@ -564,7 +550,6 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
     if (e == cudaSuccess)
       e = i8 ? i8_backward_max_pairs(&c->bwd_pairs) : tc_backward_max_pairs(ns, &c->bwd_pairs);
     if (e != cudaSuccess || c->fwd_pairs < 1 || c->bwd_pairs < 1) {
-      if (c->own_pool) cudaMemPoolDestroy(c->pool);
       delete c;
       return set_error(CCM_ERR_CUDA, "tc_forward cluster occupancy: %s", cudaGetErrorString(e));
     }
@@ -591,7 +576,6 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
     // (and torch by default) produce x and consume g
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault);
     if (e != cudaSuccess) {
-      if (c->own_pool) cudaMemPoolDestroy(c->pool);
       delete c;
       return set_error(CCM_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
     }

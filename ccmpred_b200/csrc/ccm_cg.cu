@@ -124,41 +124,40 @@ __device__ double reduce_part(const double *part, int nblocks, int k, double *re
   return t;
 }
 
-// Conditional-node values a control kernel sets.  mode 0: none (host-driven);
-// 1: the line search's WHILE only (one graph per iteration); 2: the whole solve
-// (its line search's WHILE, the IF that runs the parity-1 iteration, the outer
-// WHILE).  A kernel sets only the values of conditional nodes that enclose it
-// (their handles belong to its graph or to a graph around it); each inner WHILE
-// is re-opened by an arm kernel in the graph that holds it.
+// Conditional-node values a control kernel sets: the value of the WHILE node
+// whose body holds it (its line search) when mode >= 1.  Mode 0: none
+// (host-driven).  Every conditional value in these graphs is set in one of two
+// ways only: by a kernel in the body of a WHILE node, for that node (the
+// control and the guard), or by a kernel upstream of an IF or WHILE node in the
+// same graph (the selectors and arms).
 struct CgHandles {
-  cudaGraphConditionalHandle ls_self, it2, outer;
+  cudaGraphConditionalHandle ls_self;
   int mode, parity;
 };
 
-// Opens a WHILE node for its next execution while the solve runs.
+// Opens a WHILE node in the same graph for its next execution while the solve runs.
 __global__ void cg_arm_kernel(const CgCtl *ctl, cudaGraphConditionalHandle h) {
   cudaGraphSetConditional(h, ctl->status == kCgRunning ? 1u : 0u);
 }
 
-// First node of every round of the whole-solve graph's outer loop: counts the
-// round and opens the first line search while the solve runs.  It bounds the
-// loop on its own: past max_rounds (two iterations per round, so a solve within
-// max_iterations never gets there) it ends the solve with CCM_ERR_DEVICE and
-// closes the outer loop, whatever the other nodes did.
-__global__ void cg_guard_kernel(CgCtl *ctl, cudaGraphConditionalHandle h_out,
-                                cudaGraphConditionalHandle h_ls0, cudaGraphConditionalHandle h_it2,
-                                int max_rounds) {
+// Selects the IF node of parity p in the same graph: the solve runs and its x
+// is buffer p.
+__global__ void cg_select_kernel(const CgCtl *ctl, cudaGraphConditionalHandle h, int p) {
+  cudaGraphSetConditional(h, ctl->status == kCgRunning && ctl->parity == p ? 1u : 0u);
+}
+
+// Last node of every round of the whole-solve graph's outer loop (in its body):
+// counts the round and keeps the loop open while the solve runs.  It bounds the
+// loop on its own: past max_rounds (a round holds at least one iteration, so a
+// solve within max_iterations never gets there) it ends the solve with
+// CCM_ERR_DEVICE.
+__global__ void cg_guard_kernel(CgCtl *ctl, cudaGraphConditionalHandle h_out, int max_rounds) {
   const int round = ++ctl->rounds;
   if (ctl->status == kCgRunning && round > max_rounds) {
     ctl->status = CCM_ERR_DEVICE;
     ctl->ls_active = 0;
   }
-  const bool go = ctl->status == kCgRunning;
-  cudaGraphSetConditional(h_ls0, go ? 1u : 0u);
-  if (!go) {
-    cudaGraphSetConditional(h_it2, 0u);
-    cudaGraphSetConditional(h_out, 0u);
-  }
+  cudaGraphSetConditional(h_out, ctl->status == kCgRunning ? 1u : 0u);
 }
 
 // After the initial evaluation: f0 (from the evaluation record, or from f_slot
@@ -217,12 +216,8 @@ __global__ void __launch_bounds__(256) cg_control_kernel(CgCtl *ctl, CgRuleParam
     ctl->status = CCM_CG_ERR_LINESEARCH;
     ctl->ls_active = 0;
   }
-  const bool running = ctl->status == kCgRunning;
+  (void)accepted;
   if (h.mode >= 1) cudaGraphSetConditional(h.ls_self, ctl->ls_active ? 1u : 0u);
-  if (h.mode == 2 && (accepted || !running)) {
-    cudaGraphSetConditional(h.outer, running ? 1u : 0u);
-    if (h.parity == 0) cudaGraphSetConditional(h.it2, running ? 1u : 0u);
-  }
 }
 
 }  // namespace ccm
@@ -271,6 +266,7 @@ struct CgRun {
   cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};  // whole solve | parity 0 | parity 1
   bool want_xx = false;
   bool fused = false;
+  size_t mem_mark = 0;  // the context's mem_used before this solve's buffers
   int trial_kernels = 0;  // kernels of one trial (launch accounting)
 };
 
@@ -284,6 +280,7 @@ void free_run(CgRun &r) {
                   (void *)r.d_ctl, (void *)r.d_part})
     if (p) cudaFreeAsync(p, s);
   pinned_small_free(r.h_ctl);
+  r.c->mem_used = r.mem_mark;
 }
 
 // One trial on the stream (in capture): direction, step + evaluation, dots,
@@ -364,23 +361,22 @@ int capture_readback(CgRun &r, cudaGraph_t graph, cudaGraphNode_t dep) {
   return CCM_OK;
 }
 
-// The first node of `graph` (captured through the context's stream): an arm
-// kernel for handle h, or, with h_out, the guard of the outer loop; its node in
-// *node.
-int capture_arm(CgRun &r, cudaGraph_t graph, cudaGraphConditionalHandle h, cudaGraphNode_t *node,
-                const cudaGraphConditionalHandle *h_out = nullptr,
-                const cudaGraphConditionalHandle *h_it2 = nullptr, int max_rounds = 0) {
+// One small kernel captured into `graph` after `deps` (through the context's
+// stream); its node in *node.  kind 0: arm h; 1: select parity p on h; 2: guard.
+int capture_small(CgRun &r, cudaGraph_t graph, const cudaGraphNode_t *deps, size_t ndeps,
+                  int kind, cudaGraphConditionalHandle h, int arg, cudaGraphNode_t *node) {
   cudaStream_t s = r.c->stream;
-  cudaError_t e = cudaStreamBeginCaptureToGraph(s, graph, nullptr, nullptr, 0,
+  cudaError_t e = cudaStreamBeginCaptureToGraph(s, graph, deps, nullptr, ndeps,
                                                 cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    if (h_out) cg_guard_kernel<<<1, 1, 0, s>>>(r.d_ctl, *h_out, h, *h_it2, max_rounds);
-    else cg_arm_kernel<<<1, 1, 0, s>>>(r.d_ctl, h);
+    if (kind == 0) cg_arm_kernel<<<1, 1, 0, s>>>(r.d_ctl, h);
+    else if (kind == 1) cg_select_kernel<<<1, 1, 0, s>>>(r.d_ctl, h, arg);
+    else cg_guard_kernel<<<1, 1, 0, s>>>(r.d_ctl, h, arg);
     cudaStreamCaptureStatus cs;
-    const cudaGraphNode_t *deps = nullptr;
+    const cudaGraphNode_t *fr = nullptr;
     size_t nd = 0;
-    e = cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &nd);
-    if (e == cudaSuccess && nd == 1) *node = deps[0];
+    e = cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &fr, &nd);
+    if (e == cudaSuccess && nd == 1) *node = fr[0];
     else if (e == cudaSuccess) e = cudaErrorUnknown;
     cudaGraph_t tmp = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(s, &tmp);
@@ -390,47 +386,60 @@ int capture_arm(CgRun &r, cudaGraph_t graph, cudaGraphConditionalHandle h, cudaG
   return CCM_OK;
 }
 
+// The iteration of parity p inside the outer loop's body `b_out`, after `dep`:
+//   select(p) -> IF(sel_p) { arm -> WHILE(ls_p) { trial parity p } }
+// Its last node (the IF) in *node.
+int add_parity_iteration(CgRun &r, const CgRuleParams &rp, cudaGraph_t b_out, cudaGraphNode_t dep,
+                         int p, cudaGraphNode_t *node) {
+  cudaGraphConditionalHandle h_sel, h_ls;
+  cudaGraphNode_t n_sel, n_if, n_arm, n_ls;
+  cudaGraph_t b_if, b_ls;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h_sel, b_out, 0, cudaGraphCondAssignDefault);
+  int rc = e == cudaSuccess ? CCM_OK
+                            : set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
+  if (rc == CCM_OK) rc = capture_small(r, b_out, &dep, 1, 1, h_sel, p, &n_sel);
+  if (rc == CCM_OK) {
+    e = add_conditional(b_out, cudaGraphCondTypeIf, 0, &n_sel, 1, &h_sel, &n_if, &b_if, true);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h_ls, b_if, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) rc = set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
+  }
+  if (rc == CCM_OK) rc = capture_small(r, b_if, nullptr, 0, 0, h_ls, 0, &n_arm);
+  if (rc == CCM_OK) {
+    e = add_conditional(b_if, cudaGraphCondTypeWhile, 1, &n_arm, 1, &h_ls, &n_ls, &b_ls, true);
+    if (e != cudaSuccess) rc = set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
+  }
+  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls, p, rp, CgHandles{h_ls, 2, p});
+  *node = n_if;
+  return rc;
+}
+
 // The iteration loop of a whole solve, added to `g` after `deps`:
-//   WHILE(outer) { guard(ls0); WHILE(ls0) { trial parity 0 };
-//                  IF(it2) { arm(ls1); WHILE(ls1) { trial parity 1 } } }
+//   WHILE(outer) { select(0) -> IF { arm -> WHILE(ls0) { trial parity 0 } }
+//                  -> select(1) -> IF { arm -> WHILE(ls1) { trial parity 1 } }
+//                  -> guard }
 // The outer WHILE node's handle h_out exists already (a kernel before the loop
-// may set it).  The guard bounds the rounds by itself, so the loop ends even if
-// the line searches' nodes did not.
+// may set it).  A round runs the iteration of the parity that holds x, then the
+// other one; the guard closes the loop when the solve has ended and bounds the
+// rounds by itself.
 int add_solve_loop(CgRun &r, const CgRuleParams &rp, cudaGraph_t g,
                    cudaGraphConditionalHandle h_out, const cudaGraphNode_t *deps, size_t ndeps,
                    cudaGraphNode_t *n_out) {
-  cudaGraphConditionalHandle h_ls0, h_it2, h_ls1;
-  cudaGraphNode_t n_ls0, n_it2, n_ls1, n_arm0, n_arm1;
-  cudaGraph_t b_out = nullptr, b_ls0, b_it2, b_ls1;
+  cudaGraph_t b_out = nullptr;
   cudaGraphNodeParams np = {};
   np.type = cudaGraphNodeTypeConditional;
   np.conditional.handle = h_out;
   np.conditional.type = cudaGraphCondTypeWhile;
   np.conditional.size = 1;
   cudaError_t e = cudaGraphAddNode(n_out, g, deps, ndeps, &np);
-  if (e == cudaSuccess) b_out = np.conditional.phGraph_out[0];
-  if (e == cudaSuccess)
-    e = cudaGraphConditionalHandleCreate(&h_ls0, b_out, 1, cudaGraphCondAssignDefault);
-  if (e == cudaSuccess)
-    e = cudaGraphConditionalHandleCreate(&h_it2, b_out, 0, cudaGraphCondAssignDefault);
-  int rc = e == cudaSuccess ? CCM_OK
-                            : set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
-  if (rc == CCM_OK) rc = capture_arm(r, b_out, h_ls0, &n_arm0, &h_out, &h_it2, rp.max_iterations + 2);
-  if (rc == CCM_OK) {
-    e = add_conditional(b_out, cudaGraphCondTypeWhile, 1, &n_arm0, 1, &h_ls0, &n_ls0, &b_ls0, true);
-    if (e == cudaSuccess)
-      e = add_conditional(b_out, cudaGraphCondTypeIf, 0, &n_ls0, 1, &h_it2, &n_it2, &b_it2, true);
-    if (e == cudaSuccess)
-      e = cudaGraphConditionalHandleCreate(&h_ls1, b_it2, 1, cudaGraphCondAssignDefault);
-    if (e != cudaSuccess) rc = set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
-  }
-  if (rc == CCM_OK) rc = capture_arm(r, b_it2, h_ls1, &n_arm1);
-  if (rc == CCM_OK) {
-    e = add_conditional(b_it2, cudaGraphCondTypeWhile, 1, &n_arm1, 1, &h_ls1, &n_ls1, &b_ls1, true);
-    if (e != cudaSuccess) rc = set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
-  }
-  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls0, 0, rp, CgHandles{h_ls0, h_it2, h_out, 2, 0});
-  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls1, 1, rp, CgHandles{h_ls1, h_it2, h_out, 2, 1});
+  if (e != cudaSuccess) return set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
+  b_out = np.conditional.phGraph_out[0];
+  // an empty first node to hang the first selector on
+  cudaGraphNode_t n_start = nullptr, n_it0 = nullptr, n_it1 = nullptr, n_guard = nullptr;
+  e = cudaGraphAddEmptyNode(&n_start, b_out, nullptr, 0);
+  if (e != cudaSuccess) return set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
+  int rc = add_parity_iteration(r, rp, b_out, n_start, 0, &n_it0);
+  if (rc == CCM_OK) rc = add_parity_iteration(r, rp, b_out, n_it0, 1, &n_it1);
+  if (rc == CCM_OK) rc = capture_small(r, b_out, &n_it1, 1, 2, h_out, rp.max_iterations + 2, &n_guard);
   return rc;
 }
 
@@ -466,7 +475,7 @@ int build_iteration_graph(CgRun &r, int p, const CgRuleParams &rp) {
   e = add_conditional(g, cudaGraphCondTypeWhile, 1, nullptr, 0, &h_ls, &n_ls, &b_ls);
   int rc = e == cudaSuccess ? CCM_OK
                             : set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
-  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls, p, rp, CgHandles{h_ls, h_ls, h_ls, 1, p});
+  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls, p, rp, CgHandles{h_ls, 1, p});
   if (rc == CCM_OK) rc = capture_readback(r, g, n_ls);
   if (rc == CCM_OK) {
     e = cudaGraphInstantiate(&r.exec[1 + p], g, 0);
@@ -524,6 +533,7 @@ int ccm::cg_graph_solve_add(ccm_context *c, float *d_x, const ccm_cg_params *par
   CgGraphSolve *gs = new CgGraphSolve();
   CgRun &r = gs->r;
   r.c = c;
+  r.mem_mark = c->mem_used;
   r.n = c->nvarp;
   r.xb[0] = d_x;
   r.fused = c->path == CCM_PATH_TC_BF16X2 || c->path == CCM_PATH_TC_BF16X3 ||
@@ -649,6 +659,7 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
   const CgRuleParams rp = rule_params(*params);
   CgRun r;
   r.c = c;
+  r.mem_mark = c->mem_used;
   r.n = n;
   r.xb[0] = d_x;
   r.want_xx = progress != nullptr;
@@ -763,7 +774,7 @@ int ccm::conjugrad_callback_gpu(float *d_x, long long n, ccm_eval_callback eval,
   CgCtl *h = static_cast<CgCtl *>(pinned_small_alloc(kCgCtlHead));
   double *h_f = static_cast<double *>(pinned_small_alloc(sizeof(double)));
   if (e == cudaSuccess && (!h || !h_f)) e = cudaErrorMemoryAllocation;
-  const CgHandles none{0, 0, 0, 0, 0};
+  const CgHandles none{0, 0, 0};
   int stopped = 0;
   // one evaluation by the callback at xb[q] into gb[q]; its f goes to the device
   auto evaluate = [&](int q) -> cudaError_t {
@@ -917,6 +928,7 @@ extern "C" int ccm_conjugrad_host(ccm_context *c, float *x, long long n, const c
   if (e == cudaSuccess && rc == CCM_OK) e = cudaMemcpyAsync(x, d_x, bytes, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   cudaFreeAsync(d_x, c->stream);
+  c->mem_used -= bytes;
   if (rc != CCM_OK) return rc;
   if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "ccm_conjugrad_host: %s", cudaGetErrorString(e));
   return CCM_OK;

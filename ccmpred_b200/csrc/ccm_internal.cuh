@@ -222,7 +222,8 @@ struct ccm_context {
   int bwd_pairs = 74;             // resident CTA pairs of tc_backward
   cudaStream_t stream = nullptr;
   cudaMemPool_t pool = nullptr;   // device memory pool, or null for the device's default pool
-  bool own_pool = false;          // pool created for ccm_options.mem_limit (destroyed with the context)
+  size_t mem_limit = 0;           // ccm_options.mem_limit (0: none)
+  size_t mem_used = 0;            // device bytes held through dev_alloc_raw
   bool own_stream = false;
   int path = CCM_PATH_TC_BF16X2;
   int nsplit = 2;

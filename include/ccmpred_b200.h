@@ -86,11 +86,11 @@ typedef struct ccm_options {
 	                        that run side by side on one GPU (the batch solver) each take a
 	                        share, so that their persistent kernels stay resident together. */
 	size_t mem_limit;    /* cap on the device memory of this context, in bytes; 0 = none.
-	                        With a cap the context (and the optimizer state of
-	                        ccm_conjugrad_gpu on it) allocates from a private memory pool of
-	                        that maximum size, and an allocation beyond it fails with
-	                        CCM_ERR_NOMEM instead of taking memory that other users of the
-	                        GPU hold. */
+	                        The context counts what it allocates (its buffers, the
+	                        optimizer state of ccm_conjugrad_gpu while a solve runs, the
+	                        staging buffers of ccm_evaluate_host); an allocation beyond
+	                        the cap fails with CCM_ERR_NOMEM instead of taking memory
+	                        that other users of the GPU hold. */
 } ccm_options;
 
 /* Result of the last evaluation, as kept on the device. */

@@ -111,9 +111,9 @@ def test_non_finite_x_gives_non_finite_f(gpu, path, bad):
 
 @pytest.mark.gpu
 def test_memory_cap_gives_nomem(gpu):
-    """ccm_options.mem_limit: a private memory pool of that size backs the
-    context and its optimizer; what does not fit fails with CCM_ERR_NOMEM and
-    leaves nothing behind (the next context and evaluation work)."""
+    """ccm_options.mem_limit: the context counts the device memory it and its
+    optimizer allocate; what does not fit fails with CCM_ERR_NOMEM and leaves
+    nothing behind (the next context and evaluation work)."""
     import torch
     msa = synth.generate(synth.MSAConfig("t", 100, 1000, n_pairs=5, seed=8))
     L = 100
