@@ -154,7 +154,7 @@ __global__ void cg_select_kernel(const CgCtl *ctl, cudaGraphConditionalHandle h,
 __global__ void cg_guard_kernel(CgCtl *ctl, cudaGraphConditionalHandle h_out, int max_rounds) {
   const int round = ++ctl->rounds;
   if (ctl->status == kCgRunning && round > max_rounds) {
-    ctl->status = CCM_ERR_DEVICE;
+    ctl->status = kCgLoopBound;
     ctl->ls_active = 0;
   }
   cudaGraphSetConditional(h_out, ctl->status == kCgRunning ? 1u : 0u);
@@ -485,6 +485,15 @@ int build_iteration_graph(CgRun &r, int p, const CgRuleParams &rp) {
   return rc;
 }
 
+// CCM_ERR_DEVICE for a solve that ended on a device-side bound, with its state.
+int device_error(const char *who, const CgCtl &h) {
+  return set_last_error(CCM_ERR_DEVICE,
+                        "%s: %s (round %d, iteration %d, evaluation %d, parity %d, trial %d)", who,
+                        h.status == kCgLoopBound ? "the solve graph's round bound was reached"
+                                                 : "device wait timed out in an evaluation",
+                        h.rounds, h.iter, h.evals, h.parity, h.ls);
+}
+
 int finish(CgRun &r, float *d_x, ccm_cg_result *result, int stopped) {
   ccm_context *c = r.c;
   const CgCtl &h = *r.h_ctl;
@@ -501,12 +510,10 @@ int finish(CgRun &r, float *d_x, ccm_cg_result *result, int stopped) {
   res.evaluations = h.evals;
   res.fx = h.f;
   res.gnorm = std::sqrt(h.gg);
-  const int dev_err = h.status == CCM_ERR_DEVICE;
+  const CgCtl hc = h;
   free_run(r);
   if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "ccm_conjugrad_gpu: %s", cudaGetErrorString(e));
-  if (dev_err)
-    return set_last_error(CCM_ERR_DEVICE, "ccm_conjugrad_gpu: a device-side wait or loop bound "
-                                          "was reached (timed out in an evaluation)");
+  if (hc.status == CCM_ERR_DEVICE || hc.status == kCgLoopBound) return device_error("ccm_conjugrad_gpu", hc);
   if (result) *result = res;
   return CCM_OK;
 }
@@ -619,8 +626,7 @@ int ccm::cg_graph_solve_result(const CgGraphSolve *gs, ccm_cg_result *res) {
   res->evaluations = h.evals;
   res->fx = h.f;
   res->gnorm = std::sqrt(h.gg);
-  if (h.status == CCM_ERR_DEVICE)
-    return set_last_error(CCM_ERR_DEVICE, "ccm_solve_batch: device wait timed out in an evaluation");
+  if (h.status == CCM_ERR_DEVICE || h.status == kCgLoopBound) return device_error("ccm_solve_batch", h);
   return CCM_OK;
 }
 

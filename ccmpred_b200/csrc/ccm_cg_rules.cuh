@@ -40,6 +40,7 @@ namespace ccm {
 
 constexpr int kCgHist = 257;  // ring of accepted f: k <= 256
 constexpr int kCgRunning = 0x7fff;
+constexpr int kCgLoopBound = -1019;  // the whole-solve graph's round bound was reached
 
 struct CgRuleParams {
   int max_iterations, k, max_linesearch;
