@@ -148,9 +148,9 @@ __global__ void cg_select_kernel(const CgCtl *ctl, cudaGraphConditionalHandle h,
 
 // Last node of every round of the whole-solve graph's outer loop (in its body):
 // counts the round and keeps the loop open while the solve runs.  It bounds the
-// loop on its own: past max_rounds (a round holds at least one iteration, so a
-// solve within max_iterations never gets there) it ends the solve with
-// CCM_ERR_DEVICE.
+// loop on its own: past max_rounds (a round holds at least one trial, so a solve
+// within its trial budget never gets there) it ends the solve (reported as
+// CCM_ERR_DEVICE).
 __global__ void cg_guard_kernel(CgCtl *ctl, cudaGraphConditionalHandle h_out, int max_rounds) {
   const int round = ++ctl->rounds;
   if (ctl->status == kCgRunning && round > max_rounds) {
@@ -386,45 +386,40 @@ int capture_small(CgRun &r, cudaGraph_t graph, const cudaGraphNode_t *deps, size
   return CCM_OK;
 }
 
-// The iteration of parity p inside the outer loop's body `b_out`, after `dep`:
-//   select(p) -> IF(sel_p) { arm -> WHILE(ls_p) { trial parity p } }
-// Its last node (the IF) in *node.
-int add_parity_iteration(CgRun &r, const CgRuleParams &rp, cudaGraph_t b_out, cudaGraphNode_t dep,
-                         int p, cudaGraphNode_t *node) {
-  cudaGraphConditionalHandle h_sel, h_ls;
-  cudaGraphNode_t n_sel, n_if, n_arm, n_ls;
-  cudaGraph_t b_if, b_ls;
+// The trial of parity p inside the outer loop's body `b_out`, after `dep`:
+//   select(p) -> IF(sel_p) { trial parity p }
+// Its IF node in *node.
+int add_parity_trial(CgRun &r, const CgRuleParams &rp, cudaGraph_t b_out, cudaGraphNode_t dep,
+                     int p, cudaGraphNode_t *node) {
+  cudaGraphConditionalHandle h_sel;
+  cudaGraphNode_t n_sel, n_if;
+  cudaGraph_t b_if;
   cudaError_t e = cudaGraphConditionalHandleCreate(&h_sel, b_out, 0, cudaGraphCondAssignDefault);
   int rc = e == cudaSuccess ? CCM_OK
                             : set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
   if (rc == CCM_OK) rc = capture_small(r, b_out, &dep, 1, 1, h_sel, p, &n_sel);
   if (rc == CCM_OK) {
     e = add_conditional(b_out, cudaGraphCondTypeIf, 0, &n_sel, 1, &h_sel, &n_if, &b_if, true);
-    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h_ls, b_if, 1, cudaGraphCondAssignDefault);
     if (e != cudaSuccess) rc = set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
   }
-  if (rc == CCM_OK) rc = capture_small(r, b_if, nullptr, 0, 0, h_ls, 0, &n_arm);
-  if (rc == CCM_OK) {
-    e = add_conditional(b_if, cudaGraphCondTypeWhile, 1, &n_arm, 1, &h_ls, &n_ls, &b_ls, true);
-    if (e != cudaSuccess) rc = set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
-  }
-  if (rc == CCM_OK) rc = capture_trial_into(r, b_ls, p, rp, CgHandles{h_ls, 2, p});
+  if (rc == CCM_OK) rc = capture_trial_into(r, b_if, p, rp, CgHandles{0, 0, p});
   *node = n_if;
   return rc;
 }
 
-// The iteration loop of a whole solve, added to `g` after `deps`:
-//   WHILE(outer) { select(0) -> IF { arm -> WHILE(ls0) { trial parity 0 } }
-//                  -> select(1) -> IF { arm -> WHILE(ls1) { trial parity 1 } }
-//                  -> guard }
-// The outer WHILE node's handle h_out exists already (a kernel before the loop
-// may set it).  A round runs the iteration of the parity that holds x, then the
-// other one; the guard closes the loop when the solve has ended and bounds the
-// rounds by itself.
+// The iteration loop of a whole solve, added to `g` after `deps`, one level of
+// conditional nodes deep:
+//   WHILE(outer) { select(0) -> IF { trial parity 0 } -> select(1) -> IF { trial
+//                  parity 1 } -> guard }
+// A round takes the next trial from the buffer parity that holds x (one trial,
+// or two when the first one is accepted); the control kernels only update the
+// state record, the selectors read it, and the guard keeps the loop open while
+// the solve runs and bounds the rounds by itself.  (Line searches as WHILE
+// nodes nested inside this loop stopped iterating after a few rounds on B200
+// with driver 580; one level of IF nodes inside one WHILE does not need it.)
 int add_solve_loop(CgRun &r, const CgRuleParams &rp, cudaGraph_t g,
                    cudaGraphConditionalHandle h_out, const cudaGraphNode_t *deps, size_t ndeps,
                    cudaGraphNode_t *n_out) {
-  cudaGraph_t b_out = nullptr;
   cudaGraphNodeParams np = {};
   np.type = cudaGraphNodeTypeConditional;
   np.conditional.handle = h_out;
@@ -432,14 +427,16 @@ int add_solve_loop(CgRun &r, const CgRuleParams &rp, cudaGraph_t g,
   np.conditional.size = 1;
   cudaError_t e = cudaGraphAddNode(n_out, g, deps, ndeps, &np);
   if (e != cudaSuccess) return set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
-  b_out = np.conditional.phGraph_out[0];
-  // an empty first node to hang the first selector on
-  cudaGraphNode_t n_start = nullptr, n_it0 = nullptr, n_it1 = nullptr, n_guard = nullptr;
+  cudaGraph_t b_out = np.conditional.phGraph_out[0];
+  cudaGraphNode_t n_start = nullptr, n_t0 = nullptr, n_t1 = nullptr, n_guard = nullptr;
   e = cudaGraphAddEmptyNode(&n_start, b_out, nullptr, 0);
   if (e != cudaSuccess) return set_last_error(CCM_ERR_UNSUPPORTED, "cg graph: %s", cudaGetErrorString(e));
-  int rc = add_parity_iteration(r, rp, b_out, n_start, 0, &n_it0);
-  if (rc == CCM_OK) rc = add_parity_iteration(r, rp, b_out, n_it0, 1, &n_it1);
-  if (rc == CCM_OK) rc = capture_small(r, b_out, &n_it1, 1, 2, h_out, rp.max_iterations + 2, &n_guard);
+  // every round takes at least one trial while the solve runs; the control
+  // kernels end a solve after (max_iterations + 1) 2 (max_linesearch + 1) trials
+  const int max_rounds = (rp.max_iterations + 1) * 2 * (rp.max_linesearch + 1) + 4;
+  int rc = add_parity_trial(r, rp, b_out, n_start, 0, &n_t0);
+  if (rc == CCM_OK) rc = add_parity_trial(r, rp, b_out, n_t0, 1, &n_t1);
+  if (rc == CCM_OK) rc = capture_small(r, b_out, &n_t1, 1, 2, h_out, max_rounds, &n_guard);
   return rc;
 }
 
