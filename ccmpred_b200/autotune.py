@@ -127,10 +127,12 @@ def choose(table: Dict, L: int, N: int) -> str:
 
 
 def main():
+    import sys
+    out = sys.argv[1] if len(sys.argv) > 1 else TABLE
     table = tune()
-    with open(TABLE, "w") as f:
+    with open(out, "w") as f:
         json.dump(table, f, indent=1)
-    print(f"wrote {TABLE}")
+    print(f"wrote {out}")
 
 
 if __name__ == "__main__":
