@@ -352,11 +352,12 @@ def run_batch(args, world, rank, local):
     msas = synth.batch_workload(256, seed0=1000 + 1000 * rank)
     cb.solve_batch(msas[:2], workers=2, max_iterations=3, epsilon=1e-3, device=local)  # warm-up
     torch.cuda.synchronize()
-    # the headline: waves (one graph launch per wave), each alignment's path from the
-    # autotuner's table when it exists; beside it the same with one path for all and
-    # with host worker threads
-    runs = [("waves", "auto" if autotune.load() else args.path), ("waves", args.path),
-            ("threads", args.path)]
+    # the headline: the default host worker threads (each runs whole device-side
+    # solves), each alignment's path from the autotuner's table when it exists;
+    # beside it the same with one path for all and with waves (one graph launch
+    # per wave of alignments)
+    runs = [("threads", "auto" if autotune.load() else args.path), ("threads", args.path),
+            ("waves", args.path)]
     if runs[0] == runs[1]:
         runs = runs[1:]
     timed = {}

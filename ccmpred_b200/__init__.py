@@ -58,15 +58,16 @@ def calculate_weights(msa: np.ndarray, threshold: float = 0.8, device: int = 0) 
 
 def solve_batch(msas, workers: int = 8, path: str = "tc_i8sp", threshold: float = 0.8,
                 max_iterations: int = 250, epsilon: float = 0.01, contact_maps: bool = True,
-                device: int = 0, sms_per_worker: int = 0, waves: bool = True,
+                device: int = 0, sms_per_worker: int = 0, waves: bool = False,
                 wave_max: int = 64, wave_bytes: int = 0):
     """Solve many alignments to convergence concurrently (ccm_solve_batch).
 
     ``path="auto"`` takes each alignment's path from the table that
     ``ccmpred_b200.autotune`` measured on the GPU.
-    ``waves`` (default): one graph launch per wave of alignments (``wave_max``
-    alignments at most, ``wave_bytes`` of device memory, 0 = 60 % of the free
-    memory); else ``workers`` host threads with a context and stream each.
+    By default ``workers`` host threads with a context and stream each run the
+    alignments' device-side solves; ``waves=True``: one graph launch per wave of
+    alignments (``wave_max`` alignments at most, ``wave_bytes`` of device memory,
+    0 = 60 % of the free memory).
     Returns (results, maps): per-alignment CcmBatchResult and APC contact maps."""
     arrs = [np.ascontiguousarray(m, dtype=np.uint8) for m in msas]
     n = len(arrs)

@@ -228,7 +228,7 @@ void ccm_batch_params_default(ccm_batch_params *p) {
   p->device = 0;
   p->use_apc = 1;
   p->sms_per_worker = 0;
-  p->waves = 1;
+  p->waves = 0;
   p->wave_max = 64;
   p->wave_bytes = 0;
   ccm_cg_params_default(&p->cg);

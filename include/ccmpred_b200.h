@@ -297,12 +297,14 @@ CCM_API int ccm_conjugrad_host(ccm_context *ctx, float *x, long long n,
 /* ---------------------------------------------------------------- batched solves */
 /* Many alignments of different sizes solved to convergence concurrently on
  * one GPU (no reference counterpart: the reference runs one alignment per
- * process).  Alignments are taken largest-first.  Default (waves = 1): they are
- * admitted in waves under a device-memory budget; the whole device-side solve
- * of every alignment of a wave (initial evaluation, CG iterations in
- * conditional graph nodes, contact scores) goes into ONE graph as independent
- * branches, launched once per wave.  waves = 0: host worker threads each drive
- * their own context and stream. */
+ * process).  Alignments are taken largest-first.  Default (waves = 0): host
+ * worker threads each take the next alignment, create its context on their own
+ * stream and run its whole device-side solve (initial evaluation, CG iterations
+ * in conditional graph nodes, contact scores) as one graph launch.  waves = 1:
+ * alignments are admitted in waves under a device-memory budget and the solves
+ * of a wave go into ONE graph as independent branches, launched once per wave
+ * (a wave lasts as long as its slowest solve, so on B200 it measured a few per
+ * cent slower than the threads on the 256-alignment batch). */
 typedef struct ccm_msa_desc {
 	const unsigned char *msa;   /* nrow x ncol states 0..20, host memory */
 	int ncol;
@@ -323,8 +325,8 @@ typedef struct ccm_batch_params {
 	int sms_per_worker;          /* max_sms of every worker's contexts; 0 = no limit
 	                                (default; on B200 the 256-alignment batch ran
 	                                fastest with no limit) */
-	int waves;                   /* 1 (default): one graph launch per wave of
-	                                alignments; 0: host worker threads */
+	int waves;                   /* 0 (default): host worker threads; 1: one graph
+	                                launch per wave of alignments */
 	int wave_max;                /* most alignments in one wave (default 64) */
 	size_t wave_bytes;           /* device memory of one wave (estimated from the
 	                                alignments' sizes); 0 = 60 % of the free memory */

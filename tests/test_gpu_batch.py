@@ -16,7 +16,7 @@ def test_batch_matches_standalone_solves(gpu):
     same result: the same kernels and rules run per alignment either way."""
     msas = synth.batch_workload(10, seed0=500)
     msas = [m[: min(len(m), 1500)] for m in msas]          # keep the test short
-    resw, mapsw = solve_batch(msas, max_iterations=40, wave_max=4)
+    resw, mapsw = solve_batch(msas, max_iterations=40, waves=True, wave_max=4)
     res4, maps4 = solve_batch(msas, workers=4, max_iterations=40, waves=False)
     res1, maps1 = solve_batch(msas, workers=1, max_iterations=40, waves=False)
     for rw, r4, r1, mw, m4, m1 in zip(resw, res4, res1, mapsw, maps4, maps1):
