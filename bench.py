@@ -215,13 +215,14 @@ def max_over_ranks(world, value: float) -> float:
     return float(t.item())
 
 
-def cpu_reference_timing(msa, x, budget_s, max_evals):
-    """Reference evaluate_cpu_omp (all host threads): (evals/s, evaluations, kind, cores)."""
+def cpu_reference_timing(msa, x, budget_s, max_evals, omp=True):
+    """Reference evaluate_cpu_omp (all host threads), or with omp=False the serial
+    evaluate_cpu: (evals/s, evaluations, kind, cores)."""
     from oracle import oracle as O
     N, L = msa.shape
-    cores = os.cpu_count() or 1
+    cores = (os.cpu_count() or 1) if omp else 1
     if O.ref_available():
-        ev = O.RefEvaluator(msa, 0.01, 0.2 * (L - 1), 0.8, omp=True)
+        ev = O.RefEvaluator(msa, 0.01, 0.2 * (L - 1), 0.8, omp=omp)
         times = []
         t_start = time.perf_counter()
         try:
@@ -352,11 +353,10 @@ def run_batch(args, world, rank, local):
     msas = synth.batch_workload(256, seed0=1000 + 1000 * rank)
     cb.solve_batch(msas[:2], workers=2, max_iterations=3, epsilon=1e-3, device=local)  # warm-up
     torch.cuda.synchronize()
-    # the headline: the default host worker threads (each runs whole device-side
-    # solves), each alignment's path from the autotuner's table when it exists;
-    # beside it the same with one path for all and with waves (one graph launch
-    # per wave of alignments)
-    runs = [("threads", "auto" if autotune.load() else args.path), ("threads", args.path),
+    # the headline: solve_batch's defaults (host worker threads, each running whole
+    # device-side solves, one path for all); beside it each alignment's path from
+    # the autotuner's table, and waves (one graph launch per wave of alignments)
+    runs = [("threads", args.path), ("threads", "auto" if autotune.load() else args.path),
             ("waves", args.path)]
     if runs[0] == runs[1]:
         runs = runs[1:]
@@ -488,6 +488,18 @@ def run_large(args, world, rank, local):
     flops_eval = 4.0 * N * (21 * L) ** 2
     achieved = flops_eval * res.evaluations / (elapsed_ms / 1e3) / 1e12
     its = max(res.iterations, 1)
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        # one evaluation of the reference's evaluate_cpu_omp at the final x (about
+        # half a minute on the host cores; x, g and its per-call scratch take ~11 GB),
+        # in iterations/s at this solve's evaluations per iteration
+        v, n_ev, kind, cores = cpu_reference_timing(msa, xs.cpu().numpy(), 0.0, 1)
+        per_it = res.evaluations / its
+        cpu = {"value": v / per_it, "unit": "iterations/s", "cores": cores, "kind": kind,
+               "evals_per_s": v,
+               "sample": f"{n_ev} full evaluation of the L=1000 N=20000 workload at the final x, "
+                         f"evaluate_cpu_omp with all {cores} host threads; iterations/s at "
+                         f"{per_it:.2f} evaluations per iteration (this solve's)"}
     emit({
         "metric": f"CG iterations/s at L=1000 N=20000 ({args.cg_iterations} iterations, one "
                   "device-side solve)",
@@ -512,7 +524,7 @@ def run_large(args, world, rank, local):
             "reference": "FP64 CUDA-core path (simt_f64) at the same x"},
         "gpu_launches": int(launches), "clocks": clocks,
         "init_ms": {"weights": weights_ms},
-        "cpu_baseline": None,
+        "cpu_baseline": cpu,
     })
 
 
@@ -710,6 +722,11 @@ def main():
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
                    "sample": f"{n_ev} full evaluation(s) of the L=300 N=5000 workload "
                              f"(median), evaluate_cpu_omp with all {cores} host threads"}
+            if kind == "reference":
+                # the serial evaluate_cpu beside it (one evaluation, about 10 s)
+                v1, n1, _, _ = cpu_reference_timing(msa, x, 0.0, 1, omp=False)
+                cpu["serial_evaluate_cpu"] = {"value": v1, "unit": UNIT, "cores": 1,
+                                              "sample": f"{n1} full evaluation, evaluate_cpu"}
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
