@@ -162,3 +162,14 @@ def test_bounded_wait_runs_out(gpu, path):
         assert lib().ccm_debug_set_wait_limit(ev.handle, 0) == _lib.CCM_OK
         assert ev.evaluate(x, g) == f_ref and torch.equal(g, g_ref)
     torch.cuda.synchronize()
+
+
+def test_width_beyond_the_int_nvar_is_rejected():
+    """L = 1788 makes nvar_padded exceed the reference ABI's int nvar (2^31 - 1):
+    ccm_create refuses it before touching a device; L = 1787 is the widest."""
+    from ccmpred_b200 import nvar_padded
+    assert nvar_padded(1787) <= 0x7fffffff < nvar_padded(1788)
+    msa = np.zeros((2, 1788), np.uint8)
+    rc, ctx = create(msa)
+    assert rc == _lib.CCM_ERR_INVALID and not ctx.value
+    assert b"exceeds the int nvar" in lib().ccm_last_error()

@@ -22,7 +22,7 @@ import os
 import numpy as np
 import pytest
 
-from ccmpred_b200 import Evaluator, calculate_weights, nsingle_padded, synth
+from ccmpred_b200 import Evaluator, calculate_weights, nsingle_padded, nvar_padded, synth
 
 pytestmark = pytest.mark.gpu
 
@@ -146,3 +146,38 @@ def test_weights_above_one(gpu, oracle_mod, path, wkind):
         w = rng.choice(np.array([0.25, 1.0, 4.0], np.float32), N)
     x = synth.random_x(40, 65)
     check_paths(oracle_mod, msa, w, x, 0.01, 0.2 * 39, paths=[path])
+
+
+def test_largest_alignment_width(gpu):
+    """L = 1787, the widest alignment whose nvar_padded fits the reference ABI's int
+    (21 * 32 * L^2 coupling entries, 8.6 GB of x): every tensor-core path against the
+    FP64 CUDA-core path (itself checked against the oracle at the parity sizes) at
+    the same random admissible x, N = 64 rows.  A small lambda_pair keeps the data
+    term, not the regulariser, dominant in g."""
+    import torch
+    L, N = 1787, 64
+    msa = synth.generate(synth.MSAConfig("maxL", L, N, n_pairs=4, seed=71))
+    w = calculate_weights(msa, 0.8)
+    lam1, lam2 = 0.01, 0.01
+    nsp = nsingle_padded(L)
+    gen = torch.Generator(device="cuda").manual_seed(72)
+    x = torch.zeros(nvar_padded(L), dtype=torch.float32, device="cuda")
+    x[:20 * L] = 0.1 * torch.randn(20 * L, generator=gen, device="cuda")
+    x2 = x[nsp:].view(21, L, 32, L)
+    x2[:, :, :21, :] = 0.01 * torch.randn((21, L, 21, L), generator=gen, device="cuda")
+    idx = torch.arange(L, device="cuda")
+    x2[:, idx, :, idx] = 0.0                                # self blocks
+    with Evaluator(msa, weights=w, lambda_single=lam1, lambda_pair=lam2, path="simt_f64") as ev:
+        g64 = torch.empty(x.numel(), dtype=torch.float64, device="cuda")
+        f64 = ev.evaluate(x.double(), g64)
+    gn = torch.linalg.vector_norm(g64).item()
+    g = torch.empty_like(x)
+    for path in TC_PATHS:
+        with Evaluator(msa, weights=w, lambda_single=lam1, lambda_pair=lam2, path=path) as ev:
+            f = ev.evaluate(x, g)
+        assert torch.isfinite(g).all(), path
+        e_f = abs(f - f64) / abs(f64)
+        e = {}
+        for name, sl in (("g", slice(None)), ("g1", slice(0, 20 * L)), ("g2", slice(nsp, None))):
+            e[name] = torch.linalg.vector_norm(g[sl].double() - g64[sl]).item() / gn
+        assert e_f < 1e-6 and all(v < 1e-5 for v in e.values()), (path, e_f, e)
