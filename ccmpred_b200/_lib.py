@@ -151,6 +151,8 @@ SIGNATURES = {
                                        ctypes.POINTER(ctypes.c_int)]),
     "ccm_launch_count": (ctypes.c_longlong, [_vp]),
     "ccm_debug_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_longlong]),
+    "ccm_host_copy_bytes": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong),
+                                           ctypes.POINTER(ctypes.c_longlong)]),
     "ccm_set_default_path": (None, [ctypes.c_int]),
     "ccm_cg_params_default": (None, [ctypes.POINTER(CcmCgParams)]),
     "ccm_conjugrad_gpu": (ctypes.c_int, [_vp, _vp, ctypes.c_longlong, ctypes.POINTER(CcmCgParams),

@@ -5,8 +5,12 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
+#include <atomic>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include <cuda.h>
@@ -672,6 +676,86 @@ int ccm_evaluate(ccm_context *c, const float *d_x, float *d_g, long long nvar, d
   return CCM_OK;
 }
 
+namespace {
+
+// A few host threads that stay alive for the process, for the host-side passes
+// of ccm_evaluate_host.  parallel_for(n, f) runs f(i) for every i < n on the
+// workers and the calling thread; one job at a time.
+class HostWorkers {
+ public:
+  static HostWorkers &get() {
+    static HostWorkers w;
+    return w;
+  }
+  void parallel_for(long long n, const std::function<void(long long)> &f) {
+    std::lock_guard<std::mutex> job_lock(job_mutex_);
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      fn_ = &f;
+      n_ = n;
+      next_.store(0);
+      busy_ = (int)threads_.size();
+      ++gen_;
+    }
+    cv_.notify_all();
+    work();
+    std::unique_lock<std::mutex> lk(m_);
+    done_cv_.wait(lk, [&] { return busy_ == 0; });
+    fn_ = nullptr;
+  }
+
+ private:
+  HostWorkers() {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int n = (int)std::min(7u, hw > 1 ? hw / 2 : 1u);
+    for (int i = 0; i < n; ++i) threads_.emplace_back([this] { loop(); });
+  }
+  ~HostWorkers() {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto &t : threads_) t.join();
+  }
+  void work() {
+    for (long long i; (i = next_.fetch_add(1)) < n_;) (*fn_)(i);
+  }
+  void loop() {
+    unsigned long long seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(m_);
+        cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+      }
+      work();
+      std::lock_guard<std::mutex> lk(m_);
+      if (--busy_ == 0) done_cv_.notify_all();
+    }
+  }
+  std::vector<std::thread> threads_;
+  std::mutex job_mutex_, m_;
+  std::condition_variable cv_, done_cv_;
+  const std::function<void(long long)> *fn_ = nullptr;
+  long long n_ = 0;
+  std::atomic<long long> next_{0};
+  int busy_ = 0;
+  unsigned long long gen_ = 0;
+  bool stop_ = false;
+};
+
+}  // namespace
+
+// Host x and g.  The padding states a in [21, 32) of the coupling block are 34 %
+// of x and are zero on every path that starts from init_bias or a .raw file
+// (src/ccmpred.c:101, src/io.c:81-95); where they are zero (checked on the host,
+// bit patterns, while the DMA copies the rest) neither they nor the gradient's
+// padding states (2 lambda2 x = 0) cross PCIe: x and g move as 21 L rows of 21 L
+// floats with a pitch of 32 L, and the host writes g's padding states as zeros
+// during the device-to-host copy.  Any nonzero bit there: the padding is copied
+// both ways as well.
 int ccm_evaluate_host(ccm_context *c, const float *x, float *g, long long nvar, double *fx) {
   if (!c || !x || !g) return set_error(CCM_ERR_INVALID, "ccm_evaluate_host: null argument");
   if (nvar != c->nvarp)
@@ -680,15 +764,62 @@ int ccm_evaluate_host(ccm_context *c, const float *x, float *g, long long nvar, 
   if (!c->d_xh) {
     CCM_CUDA_TRY(dev_alloc(c, &c->d_xh, bytes));
     CCM_CUDA_TRY(dev_alloc(c, &c->d_gh, bytes));
+    CCM_CUDA_TRY(cudaMemsetAsync(c->d_xh, 0, bytes, c->stream));
+    c->xh_pad_dirty = false;
   }
-  CCM_CUDA_TRY(cudaMemcpyAsync(c->d_xh, x, bytes, cudaMemcpyHostToDevice, c->stream));
+  const int L = c->L;
+  const long long nsp = c->nsp, rows = (long long)kQ * L;
+  const size_t pitch = sizeof(float) * kQPad * (size_t)L;
+  const size_t real = sizeof(float) * kQ * (size_t)L, pad = pitch - real;
+  // single fields, then the 21 states of every row
+  CCM_CUDA_TRY(cudaMemcpyAsync(c->d_xh, x, sizeof(float) * nsp, cudaMemcpyHostToDevice, c->stream));
+  CCM_CUDA_TRY(cudaMemcpy2DAsync(c->d_xh + nsp, pitch, x + nsp, pitch, real, rows,
+                                 cudaMemcpyHostToDevice, c->stream));
+  long long h2d = sizeof(float) * nsp + (long long)real * rows;
+  std::atomic<int> nonzero{0};
+  const long long kRowsPerJob = 64;
+  HostWorkers::get().parallel_for((rows + kRowsPerJob - 1) / kRowsPerJob, [&](long long job) {
+    uint32_t acc = 0;
+    for (long long r = job * kRowsPerJob; r < std::min(rows, (job + 1) * kRowsPerJob); ++r) {
+      const uint32_t *p = reinterpret_cast<const uint32_t *>(x + nsp + r * kQPad * L + kQ * L);
+      for (size_t i = 0; i < pad / 4; ++i) acc |= p[i];
+    }
+    if (acc) nonzero.store(1, std::memory_order_relaxed);
+  });
+  const bool pad_nonzero = nonzero.load() != 0;
+  if (pad_nonzero) {
+    CCM_CUDA_TRY(cudaMemcpy2DAsync(c->d_xh + nsp + kQ * L, pitch, x + nsp + kQ * L, pitch, pad, rows,
+                                   cudaMemcpyHostToDevice, c->stream));
+    h2d += (long long)pad * rows;
+  } else if (c->xh_pad_dirty) {
+    CCM_CUDA_TRY(cudaMemset2DAsync(c->d_xh + nsp + kQ * L, pitch, 0, pad, rows, c->stream));
+  }
+  c->xh_pad_dirty = pad_nonzero;
   int rc = enqueue_eval(c, c->d_xh, c->d_gh);
   if (rc != CCM_OK) return rc;
-  CCM_CUDA_TRY(cudaMemcpyAsync(g, c->d_gh, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CCM_CUDA_TRY(cudaMemcpyAsync(g, c->d_gh, sizeof(float) * nsp, cudaMemcpyDeviceToHost, c->stream));
+  CCM_CUDA_TRY(cudaMemcpy2DAsync(g + nsp, pitch, c->d_gh + nsp, pitch, pad_nonzero ? pitch : real,
+                                 rows, cudaMemcpyDeviceToHost, c->stream));
+  long long d2h = sizeof(float) * nsp + (long long)(pad_nonzero ? pitch : real) * rows;
   CCM_CUDA_TRY(cudaMemcpyAsync(c->h_out, c->d_out, sizeof(ccm_result), cudaMemcpyDeviceToHost, c->stream));
+  d2h += sizeof(ccm_result);
+  if (!pad_nonzero)  // g's padding states, disjoint from what the copy writes
+    HostWorkers::get().parallel_for((rows + kRowsPerJob - 1) / kRowsPerJob, [&](long long job) {
+      for (long long r = job * kRowsPerJob; r < std::min(rows, (job + 1) * kRowsPerJob); ++r)
+        std::memset(g + nsp + r * kQPad * L + kQ * L, 0, pad);
+    });
   CCM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->host_h2d = h2d;
+  c->host_d2h = d2h;
   if ((rc = check_status(c)) != CCM_OK) return rc;
   if (fx) *fx = c->h_out->fx;
+  return CCM_OK;
+}
+
+int ccm_host_copy_bytes(const ccm_context *c, long long *h2d, long long *d2h) {
+  if (!c || !h2d || !d2h) return set_error(CCM_ERR_INVALID, "ccm_host_copy_bytes: null argument");
+  *h2d = c->host_h2d;
+  *d2h = c->host_d2h;
   return CCM_OK;
 }
 

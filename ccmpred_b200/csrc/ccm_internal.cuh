@@ -276,6 +276,8 @@ struct ccm_context {
 
   // host-pointer evaluation scratch
   float *d_xh = nullptr, *d_gh = nullptr;
+  bool xh_pad_dirty = false;           // d_xh holds nonzero padding states
+  long long host_h2d = 0, host_d2h = 0;  // bytes the last ccm_evaluate_host copied
 
   // instrumentation
   long long launches = 0;              // kernels launched by this context

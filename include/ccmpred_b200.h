@@ -145,9 +145,14 @@ CCM_API int ccm_evaluate(ccm_context *ctx, const float *d_x, float *d_g, long lo
 CCM_API int ccm_evaluate_async(ccm_context *ctx, const float *d_x, float *d_g, long long nvar_padded);
 
 /* Same with HOST x and g (the evaluate_cpu convention, src/evaluate_cpu.c:16-166):
- * copies x in, evaluates, copies g out. */
+ * copies x in, evaluates, copies g out.  Where the padding states a in [21, 32)
+ * of x's coupling block are all zero bits (always on the reference's CLI path),
+ * they and g's padding states (then zero) do not cross PCIe: the host checks
+ * them while the rest is copied and writes g's as zeros. */
 CCM_API int ccm_evaluate_host(ccm_context *ctx, const float *x, float *g, long long nvar_padded,
                       double *fx);
+/* Bytes the last ccm_evaluate_host copied host -> device and device -> host. */
+CCM_API int ccm_host_copy_bytes(const ccm_context *ctx, long long *h2d, long long *d2h);
 
 /* FP64 evaluation (CCM_PATH_SIMT_F64 contexts): double x and g on the device. */
 CCM_API int ccm_evaluate_f64(ccm_context *ctx, const double *d_x, double *d_g, long long nvar_padded,

@@ -196,3 +196,36 @@ def test_long_alignment_against_f64_path(gpu, path):
     ev.close()
     e = errors(f, g.cpu().numpy(), f64, g64.cpu().numpy(), L)
     assert within(e, TOL[path]), e
+
+
+@pytest.mark.parametrize("path", ["tc_i8sp", "simt_f32"])
+def test_host_pointer_evaluation_and_padding(gpu, path):
+    """ccm_evaluate_host equals the device-pointer evaluation bit for bit in every
+    case of its padding rule: zero padding states (they and g's stay off PCIe, g's
+    written as zeros on the host: fewer bytes copied), nonzero padding (an
+    inadmissible x: copied both ways), zero again after that (the device copy's
+    padding cleared), and -0.0 in the padding (a nonzero bit pattern: copied)."""
+    import torch
+    L, N = 37, 300
+    msa = synth.generate(synth.MSAConfig("hp", L, N, n_pairs=3, seed=41))
+    nsp = 20 * L + 32 - (20 * L) % 32
+    x0 = synth.random_x(L, 42)
+    x1 = x0.copy()
+    x1[nsp:].reshape(21, L, 32, L)[:, :, 21:, :] = 0.01 * np.random.default_rng(43).standard_normal(
+        (21, L, 11, L)).astype(np.float32)
+    x2 = x0.copy()
+    x2[nsp + 5 * 32 * L + 21 * L + 3] = -0.0
+    real = 4 * (nsp + 21 * L * 21 * L)
+    full = 4 * x0.size
+    with Evaluator(msa, path=path) as ev:
+        for x, h2d_expected in ((x0, real), (x1, full), (x0, real), (x2, full)):
+            xd = torch.from_numpy(x).cuda()
+            gd = torch.empty_like(xd)
+            f_dev = ev.evaluate(xd, gd)
+            gh = np.full_like(x, np.nan)
+            f_host = ev.evaluate(np.ascontiguousarray(x), gh)
+            assert f_host == f_dev
+            assert np.array_equal(gh.view(np.uint32), gd.cpu().numpy().view(np.uint32))
+            h2d, d2h = ctypes.c_longlong(), ctypes.c_longlong()
+            assert lib().ccm_host_copy_bytes(ev.handle, ctypes.byref(h2d), ctypes.byref(d2h)) == 0
+            assert h2d.value == h2d_expected and d2h.value == h2d_expected + 32
