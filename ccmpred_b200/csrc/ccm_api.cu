@@ -509,9 +509,10 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
     return set_error(CCM_ERR_INVALID, "ccm_create: unknown gradient mode %d", o.gradient);
   for (long long i = 0; i < (long long)ncol * nrow; ++i)
     if (msa[i] > 20) return set_error(CCM_ERR_INVALID, "ccm_create: MSA state %d > 20 at %lld", msa[i], i);
-  // the integer paths encode R = w (P - onehot) with 21 fractional bits below a
-  // power-of-two scale 2^eR >= max |w|
-  float wmax = 1.0f;
+  // the integer paths encode R = w (P - onehot), |R| <= max |w|, with 21
+  // fractional bits below the smallest power of two 2^eR >= max |w| (below 1 too:
+  // an alignment whose rows all carry small weights keeps its residuals' bits)
+  float wmax = weights ? 0.0f : 1.0f;
   if (weights)
     for (int i = 0; i < nrow; ++i) {
       if (!std::isfinite(weights[i]))
@@ -519,10 +520,11 @@ int ccm::create_context(ccm_context **out, const unsigned char *msa, int ncol, i
       wmax = std::max(wmax, std::fabs(weights[i]));
     }
   int r_exp = 0;
-  if (wmax > 1.0f) {
+  if (wmax > 0.0f) {
     (void)std::frexp(wmax, &r_exp);                   // wmax = m 2^r_exp, m in [0.5, 1)
     if (std::ldexp(1.0f, r_exp - 1) == wmax) --r_exp;  // an exact power of two
     if (r_exp > 100) return set_error(CCM_ERR_INVALID, "ccm_create: weight %g too large", wmax);
+    r_exp = std::max(r_exp, -100);
   }
   // the coupling block has 21*32*L^2 entries; keep every index in 32-bit range of int callers
   if (nvar_padded_of(ncol) > 0x7fffffffLL)

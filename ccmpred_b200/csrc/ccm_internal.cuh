@@ -67,8 +67,8 @@ struct I8FwdArgs {
   int *status;
   int L, N, S, T, Npad, m_tiles;
   int KP;  // sparse forward: logical K (a multiple of 256)
-  // digits of R: R * r_enc with r_enc = 2^(21 - eR), eR = ceil(log2 max |w|) for
-  // weights above 1, else 0, so that |R| <= max |w| stays within 21 bits
+  // digits of R: R * r_enc with r_enc = 2^(21 - eR), eR = ceil(log2 max |w|) (0 for
+  // uniform weights), so that |R| <= max |w| fills, and stays within, 21 bits
   float r_enc;
   // > 0: instead of waiting for a finished accumulator, the epilogue waits this
   // many clock cycles on a barrier that nothing arrives on, so that the wait runs
@@ -231,7 +231,7 @@ struct ccm_context {
 
   int L = 0, N = 0;
   long long nsingle = 0, nsp = 0, nvarp = 0;
-  int r_exp = 0;                   // eR of the integer path's R digits (weights above 1)
+  int r_exp = 0;                   // eR of the integer path's R digits: 2^eR >= max |w|
   long long acc_wait_cycles = 0;   // ccm_debug_set_wait_limit (0: default budget)
   float lambda_single = 0.01f, lambda_pair = 0.0f;
 

@@ -126,8 +126,8 @@ CCM_API void ccm_options_default(ccm_options *opt, int ncol);
 
 /* Upload the alignment and weights, allocate all device state for `path`.
  * weights == NULL means uniform weights 1.0 (src/reweighting.c:61-67); weights
- * must be finite (any magnitude: the integer paths scale the residuals by a
- * power of two when a weight exceeds 1).  States above 20 are rejected with
+ * must be finite (any magnitude: the integer paths scale the residuals by the
+ * smallest power of two at or above the largest weight).  States above 20 are rejected with
  * CCM_ERR_INVALID.  Replaces init_cuda (src/evaluate_cuda.c:77-139) without
  * process globals. */
 CCM_API int ccm_create(ccm_context **ctx, const unsigned char *msa, int ncol, int nrow,

@@ -78,6 +78,8 @@ CASES = [
     ("L75_N1000_rand", synth.SMALL_75x1000, "rand"),
     ("L13_N64_rand", synth.MSAConfig("t", 13, 64, n_pairs=3, seed=13), "rand"),
     ("L1_N9_rand", synth.MSAConfig("t", 1, 9, seed=14), "rand"),
+    ("L7_N1_rand", synth.MSAConfig("t", 7, 1, seed=15), "rand"),
+    ("L2_N2_bias", synth.MSAConfig("t", 2, 2, seed=16), "bias"),
     ("L150_N2000_rand", synth.AUTOGRAD_150x2000, "rand"),
 ]
 
@@ -98,6 +100,34 @@ def test_synthetic(gpu, oracle_mod, path, name, cfg, xkind):
     f64, g64 = oracle_mod.oracle_evaluate(msa, w, lam1, lam2, x)
     e = errors(f, g, f64, g64, L)
     assert within(e, TOL[path]), e
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("kind", ["all_gap", "conserved", "one_state_per_row"])
+def test_degenerate_alignments(gpu, oracle_mod, path, kind):
+    """Alignments the generator does not produce: every state a gap, every
+    column conserved (one state throughout, so P is near one-hot and R small), and
+    every row a single repeated state (one-hot slots of one state only)."""
+    L, N = 20, 60
+    rng = np.random.default_rng(17)
+    if kind == "all_gap":
+        msa = np.full((N, L), 20, np.uint8)
+    elif kind == "conserved":
+        msa = np.tile(rng.integers(0, 21, L, dtype=np.uint8), (N, 1))
+    else:
+        msa = np.repeat(rng.integers(0, 21, (N, 1), dtype=np.uint8), L, axis=1)
+    w = oracle_mod.oracle_weights(msa, 0.8)
+    for xkind in ("bias", "rand"):
+        if xkind == "bias":
+            from ccmpred_b200.host import init_bias
+            x = init_bias(msa)
+        else:
+            x = synth.random_x(L, 18)
+        f, g = run(path, msa, w, x, 0.01, 0.2 * (L - 1))
+        assert np.all(np.isfinite(g))
+        f64, g64 = oracle_mod.oracle_evaluate(msa, w, 0.01, 0.2 * (L - 1), x)
+        e = errors(f, g, f64, g64, L)
+        assert within(e, TOL[path]), (xkind, e)
 
 
 @pytest.mark.parametrize("path", ["tc_bf16x2", "tc_i8x3", "tc_i8sp", "simt_f32"])
