@@ -282,6 +282,9 @@ int alloc_tc(ccm_context *c) {
   const long long fwd_tiles = (long long)(c->Npad / 128) * c->T;
   CCM_CUDA_TRY(dev_alloc(c, &c->d_part_f, sizeof(double) * fwd_tiles * 8));
   CCM_CUDA_TRY(dev_alloc(c, &c->d_part_reg, sizeof(double) * kQ * c->L));
+  CCM_CUDA_TRY(dev_alloc(c, &c->d_fin_part, sizeof(double) * 3 * kFinBlocks));
+  CCM_CUDA_TRY(dev_alloc(c, &c->d_fin_done, sizeof(unsigned)));
+  CCM_CUDA_TRY(cudaMemsetAsync(c->d_fin_done, 0, sizeof(unsigned), c->stream));
   CCM_CUDA_TRY(dev_alloc(c, &c->d_g1d, sizeof(float) * (kQ - 1) * c->L));
 
   std::vector<int2> tiles;
@@ -367,7 +370,7 @@ void free_all(ccm_context *c) {
   f(c->d_msa); f(c->d_w); f(c->d_out); f(c->d_onehot);
   for (int i = 0; i < 3; ++i) { f(c->d_wperm[i]); f(c->d_r[i]); f(c->d_wdig[i]); f(c->d_rdig[i]); }
   f(c->d_o1); f(c->d_o128); f(c->d_colmax); f(c->d_ac1); f(c->d_ac128); f(c->d_meta);
-  f(c->d_part_f); f(c->d_part_reg); f(c->d_g1d); f(c->d_bwd_tiles);
+  f(c->d_part_f); f(c->d_part_reg); f(c->d_fin_part); f(c->d_fin_done); f(c->d_g1d); f(c->d_bwd_tiles);
   f(c->d_simt_pc); f(c->d_simt_g2); f(c->d_simt_part); f(c->d_simt_g1);
   f(c->d_xh); f(c->d_gh);
   if (c->h_out) pinned_small_free(c->h_out);

@@ -123,7 +123,10 @@ struct FinalizeArgs {
   int L;
   float lambda_single, lambda_pair;
   ccm_result *out;
+  double *block_part;  // kFinBlocks x 3 sums
+  unsigned *done;      // blocks finished (0 between evaluations)
 };
+constexpr int kFinBlocks = 16, kFinThreads = 512;
 
 // Per-kernel CUDA-event timing of evaluations (ccm_profile_begin/end): one
 // event before the first kernel of an evaluation and one after each kernel.
@@ -249,6 +252,8 @@ struct ccm_context {
   __nv_bfloat16 *d_r[3] = {nullptr, nullptr, nullptr};      // Npad x S
   double *d_part_f = nullptr;
   double *d_part_reg = nullptr;
+  double *d_fin_part = nullptr;     // tc_finalize: per-block sums
+  unsigned *d_fin_done = nullptr;   // tc_finalize: its ticket counter
   float *d_g1d = nullptr;                // 20 L single-field data gradient
   int2 *d_bwd_tiles = nullptr;
   int n_bwd_tiles = 0;

@@ -812,15 +812,20 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kBwdThreads, 1)
 // -------------------------------------------------------------- tc_finalize
 // fx = sum(loss partials) + lambda1 sum V^2 + 0.5 lambda2 sum x2^2 (all in FP64,
 // fixed summation order); g1 = g1d + 2 lambda1 V, g1 padding = 0
-// (src/evaluate_cpu.c:151-163).
-__global__ void __launch_bounds__(1024) tc_finalize_kernel(FinalizeArgs args) {
-  __shared__ double red[32];
+// (src/evaluate_cpu.c:151-163).  kFinBlocks blocks each sum a fixed share of
+// the partials; the block that finishes last (a ticket counter, reset by it)
+// adds the blocks' sums in block order and writes the result.
+__global__ void __launch_bounds__(kFinThreads) tc_finalize_kernel(FinalizeArgs args) {
+  __shared__ double red[kFinThreads / 32][3];
+  __shared__ bool last;
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
   double acc_f = 0.0, acc_r2 = 0.0, acc_r1 = 0.0;
-  for (long long i = threadIdx.x; i < args.n_part_f; i += blockDim.x) acc_f += args.part_f[i];
-  for (long long i = threadIdx.x; i < args.n_part_reg; i += blockDim.x) acc_r2 += args.part_reg[i];
+  for (long long i = tid; i < args.n_part_f; i += stride) acc_f += args.part_f[i];
+  for (long long i = tid; i < args.n_part_reg; i += stride) acc_r2 += args.part_reg[i];
   const long long ns = nsingle_of(args.L);
   const float two_l1 = 2.0f * args.lambda_single;
-  for (long long v = threadIdx.x; v < args.nsp; v += blockDim.x) {
+  for (long long v = tid; v < args.nsp; v += stride) {
     if (v < ns) {
       const float xv = args.x1[v];
       acc_r1 += (double)xv * (double)xv;
@@ -829,24 +834,33 @@ __global__ void __launch_bounds__(1024) tc_finalize_kernel(FinalizeArgs args) {
       args.g1[v] = 0.0f;
     }
   }
-  auto block_sum = [&](double x) -> double {
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
-    __syncthreads();
-    double s = 0.0;
-    if (threadIdx.x == 0)
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-    return s;
-  };
-  const double F = block_sum(acc_f);
-  const double R2 = block_sum(acc_r2);
-  const double R1 = block_sum(acc_r1);
+  double acc[3] = {acc_f, acc_r2, acc_r1};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][k] = acc[k];
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+      for (int k = 0; k < 3; ++k) s[k] += red[w][k];
+    for (int k = 0; k < 3; ++k) args.block_part[3 * blockIdx.x + k] = s[k];
+    __threadfence();
+    last = atomicAdd(args.done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int b = 0; b < (int)gridDim.x; ++b)
+      for (int k = 0; k < 3; ++k) s[k] += __ldcg(args.block_part + 3 * b + k);
+    const double F = s[0], R2 = s[1], R1 = s[2];
     const double fx = F + (double)args.lambda_single * R1 + 0.5 * (double)args.lambda_pair * R2;
     args.out->fx = fx;
     args.out->f_data = F;
     args.out->reg = fx - F;
+    *args.done = 0u;  // for the next evaluation (also inside a replayed graph)
   }
 }
 
@@ -915,7 +929,8 @@ cudaError_t launch_tc_finalize(ccm_context *c, const float *x1, float *d_g, long
   za.part_reg = c->d_part_reg; za.n_part_reg = (long long)kQ * c->L;
   za.x1 = x1; za.g1d = c->d_g1d; za.g1 = d_g; za.L = c->L; za.nsp = c->nsp;
   za.lambda_single = c->lambda_single; za.lambda_pair = c->lambda_pair; za.out = c->d_out;
-  tc_finalize_kernel<<<1, 1024, 0, c->stream>>>(za);
+  za.block_part = c->d_fin_part; za.done = c->d_fin_done;
+  tc_finalize_kernel<<<kFinBlocks, kFinThreads, 0, c->stream>>>(za);
   return cudaGetLastError();
 }
 
