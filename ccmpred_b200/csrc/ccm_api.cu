@@ -18,6 +18,7 @@
 
 #include "ccm_internal.cuh"
 #include "ccm_layout.cuh"
+#include "ccm_ptx.cuh"
 
 namespace ccm {
 
@@ -33,6 +34,8 @@ void count_launch(ccm_context *c, int n) { c->launches += n; }
 // evaluation is also captured into the bodies of conditional graph nodes (the
 // device-side CG), which hold kernel nodes.
 __global__ void zero_words_kernel(uint32_t *__restrict__ p, long long words) {
+  griddep_wait();
+  griddep_launch();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < words;
        i += (long long)gridDim.x * blockDim.x)
     p[i] = 0u;
@@ -40,9 +43,8 @@ __global__ void zero_words_kernel(uint32_t *__restrict__ p, long long words) {
 
 cudaError_t zero_words(void *p, long long words, cudaStream_t s) {
   const long long blocks = (words + 255) / 256;
-  zero_words_kernel<<<(unsigned)(blocks < 1184 ? (blocks > 0 ? blocks : 1) : 1184), 256, 0, s>>>(
-      static_cast<uint32_t *>(p), words);
-  return cudaGetLastError();
+  return launch_pdl(zero_words_kernel, dim3((unsigned)(blocks < 1184 ? (blocks > 0 ? blocks : 1) : 1184)),
+                    dim3(256), 0, s, static_cast<uint32_t *>(p), words);
 }
 
 bool is_context(const void *p) {

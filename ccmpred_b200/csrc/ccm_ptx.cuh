@@ -74,6 +74,18 @@ __device__ __forceinline__ void tma_load_2d(void *smem_dst, const CUtensorMap *m
       : "memory");
 }
 
+// Programmatic dependent launch.  griddep_wait: block until the previous kernel
+// of the stream has completed and its writes are visible (a no-op for a kernel
+// launched without the attribute); every kernel of the evaluation calls it before
+// its first global-memory access.  griddep_launch: every CTA issues it when it
+// starts; the next kernel of the stream is scheduled once all CTAs of this one
+// have (its CTAs then take free SMs and wait in griddep_wait), so it never holds
+// a slot that a CTA of this kernel still needs.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ void prefetch_tmap(const CUtensorMap *map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }

@@ -818,6 +818,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kBwdThreads, 1)
 __global__ void __launch_bounds__(kFinThreads) tc_finalize_kernel(FinalizeArgs args) {
   __shared__ double red[kFinThreads / 32][3];
   __shared__ bool last;
+  griddep_wait();
+  griddep_launch();
   const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long stride = (long long)gridDim.x * blockDim.x;
   double acc_f = 0.0, acc_r2 = 0.0, acc_r1 = 0.0;
@@ -930,8 +932,7 @@ cudaError_t launch_tc_finalize(ccm_context *c, const float *x1, float *d_g, long
   za.x1 = x1; za.g1d = c->d_g1d; za.g1 = d_g; za.L = c->L; za.nsp = c->nsp;
   za.lambda_single = c->lambda_single; za.lambda_pair = c->lambda_pair; za.out = c->d_out;
   za.block_part = c->d_fin_part; za.done = c->d_fin_done;
-  tc_finalize_kernel<<<kFinBlocks, kFinThreads, 0, c->stream>>>(za);
-  return cudaGetLastError();
+  return launch_pdl(tc_finalize_kernel, dim3(kFinBlocks), dim3(kFinThreads), 0, c->stream, za);
 }
 
 cudaError_t tc_backward_max_pairs(int nsplit, int *pairs) {

@@ -71,6 +71,8 @@ __global__ void __launch_bounds__(256) i8_colmax_kernel(const float *__restrict_
                                                         uint32_t *__restrict__ colmax, int L,
                                                         long long nsp, int rows_per_block,
                                                         int krow_order) {
+  griddep_wait();
+  griddep_launch();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int w32 = kQPad * L;
   float a = 0.0f;
@@ -108,6 +110,8 @@ __global__ void __launch_bounds__(256) i8_colmax_kernel(const float *__restrict_
 template <class G>
 __global__ void i8_scales_kernel(const uint32_t *__restrict__ colmax, float *__restrict__ enc,
                                  int L, int S) {
+  griddep_wait();
+  griddep_launch();
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= S) return;
   const int t = s / G::kSlots, r = s % G::kSlots;
@@ -161,6 +165,8 @@ __host__ __device__ constexpr long long i8sp_b_offset(int kr, int s, int KB) {
 template <class G, bool NAT>
 __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ x2,
                                                       float *__restrict__ g2, I8PrepArgs args) {
+  griddep_wait();
+  griddep_launch();
   extern __shared__ __align__(16) float xrow[];  // S floats: the row in slot order
   const int L = args.L;
   // NAT: blocks in K-row order k * 21 + b, so that blocks running together fill
@@ -589,6 +595,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
   tc_fence_before();
   cluster_sync();
   tc_fence_after();
+  // the prologue above overlaps the previous kernel's tail; its outputs from here
+  griddep_launch();
+  griddep_wait();
   const uint32_t tmem_base = *tmem_slot;
   const uint32_t t_hi = tmem_base, t_lo = tmem_base + kI8BN;
 
@@ -886,6 +895,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
   tc_fence_before();
   cluster_sync();
   tc_fence_after();
+  // the prologue above overlaps the previous kernel's tail; its outputs from here
+  griddep_launch();
+  griddep_wait();
   const uint32_t tmem_base = *tmem_slot;
   // TMEM: hi [0, 192), the epilogue's stash [192, 256), lo [256, 448), metadata 448 / 452
   const uint32_t t_hi = tmem_base, t_lo = tmem_base + 256, t_e = tmem_base + 448;
@@ -1102,6 +1114,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
   tc_fence_before();
   cluster_sync();
   tc_fence_after();
+  // the prologue above overlaps the previous kernel's tail; its outputs from here
+  griddep_launch();
+  griddep_wait();
   const uint32_t tmem_base = *tmem_slot;
   const uint32_t t_hi = tmem_base, t_lo = tmem_base + kBN;
 
@@ -1331,22 +1346,24 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   constexpr int kRows = 32;
   const dim3 cgrid((kQPad * L + 255) / 256, (kQ * L + kRows - 1) / kRows + (step ? 1 : 0));
   if (step)
-    i8_colmax_kernel<true><<<cgrid, 256, 0, c->stream>>>(d_x, d_s, d_alpha, d_xt, c->d_colmax,
-                                                          L, c->nsp, kRows, sp ? 1 : 0);
+    e = launch_pdl(i8_colmax_kernel<true>, cgrid, dim3(256), 0, c->stream, d_x, d_s, d_alpha, d_xt,
+                   c->d_colmax, L, c->nsp, kRows, sp ? 1 : 0);
   else
-    i8_colmax_kernel<false><<<cgrid, 256, 0, c->stream>>>(d_x, nullptr, nullptr, nullptr,
-                                                           c->d_colmax, L, c->nsp, kRows,
-                                                           sp ? 1 : 0);
+    e = launch_pdl(i8_colmax_kernel<false>, cgrid, dim3(256), 0, c->stream, d_x,
+                   (const float *)nullptr, (const double *)nullptr, (float *)nullptr, c->d_colmax,
+                   L, c->nsp, kRows, sp ? 1 : 0);
+  if (e != cudaSuccess) return e;
   // per-slot factors after the column maxima, 16-byte aligned for the float4 loads
   float *enc = reinterpret_cast<float *>(c->d_colmax + ((kQ * L + 3) & ~3));
   // W digit rows: S slots (dense forward) or SW slots of 192-slot groups (sparse)
   const int wcols = sp ? c->SW : c->S;
   if (sp)
-    i8_scales_kernel<Groups192><<<(wcols + 255) / 256, 256, 0, c->stream>>>(c->d_colmax, enc, L,
-                                                                             wcols);
+    e = launch_pdl(i8_scales_kernel<Groups192>, dim3((wcols + 255) / 256), dim3(256), 0, c->stream,
+                   (const uint32_t *)c->d_colmax, enc, L, wcols);
   else
-    i8_scales_kernel<Groups256><<<(wcols + 255) / 256, 256, 0, c->stream>>>(c->d_colmax, enc, L,
-                                                                             wcols);
+    e = launch_pdl(i8_scales_kernel<Groups256>, dim3((wcols + 255) / 256), dim3(256), 0, c->stream,
+                   (const uint32_t *)c->d_colmax, enc, L, wcols);
+  if (e != cudaSuccess) return e;
   I8PrepArgs pa{};
   for (int i = 0; i < 3; ++i) pa.wdig[i] = c->d_wdig[i];
   pa.colmax = c->d_colmax;
@@ -1356,9 +1373,12 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   pa.g2_coef = c->gradient == CCM_GRADIENT_PARTIAL ? 1.0f : 2.0f;
   pa.inv_L = 1.0f / (float)L;
   if (sp)
-    i8_prep_kernel<Groups192, true><<<kQ * L, 256, sizeof(float) * wcols, c->stream>>>(x2, g2, pa);
+    e = launch_pdl(i8_prep_kernel<Groups192, true>, dim3(kQ * L), dim3(256), sizeof(float) * wcols,
+                   c->stream, x2, g2, pa);
   else
-    i8_prep_kernel<Groups256, false><<<kQ * L, 256, sizeof(float) * wcols, c->stream>>>(x2, g2, pa);
+    e = launch_pdl(i8_prep_kernel<Groups256, false>, dim3(kQ * L), dim3(256), sizeof(float) * wcols,
+                   c->stream, x2, g2, pa);
+  if (e != cudaSuccess) return e;
   prof_mark(c);
 
   I8FwdArgs fa{};
@@ -1373,9 +1393,12 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   const int pair_tiles = fa.m_tiles * c->T;
   const int fpairs = pair_tiles < c->fwd_pairs ? pair_tiles : c->fwd_pairs;
   if (sp)
-    i8sp_forward_kernel<<<2 * fpairs, kI8Threads, I8SpSmem::kTotal, c->stream>>>(c->i8sp_maps, fa);
+    e = launch_pdl(i8sp_forward_kernel, dim3(2 * fpairs), dim3(kI8Threads), I8SpSmem::kTotal,
+                   c->stream, c->i8sp_maps, fa);
   else
-    i8_forward_kernel<<<2 * fpairs, kI8Threads, I8FwdSmem::kTotal, c->stream>>>(c->i8fwd_maps, fa);
+    e = launch_pdl(i8_forward_kernel, dim3(2 * fpairs), dim3(kI8Threads), I8FwdSmem::kTotal,
+                   c->stream, c->i8fwd_maps, fa);
+  if (e != cudaSuccess) return e;
   prof_mark(c);
 
   BwdArgs ba{};
@@ -1386,21 +1409,15 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   const int bpairs = c->n_bwd_tiles < c->bwd_pairs ? c->n_bwd_tiles : c->bwd_pairs;
   const bool sym = c->gradient != CCM_GRADIENT_PARTIAL;
   const dim3 bgrid(2 * bpairs);
-  if (sp && sym)
-    i8_backward_kernel<true, Groups192, true>
-        <<<bgrid, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
-  else if (sp)
-    i8_backward_kernel<false, Groups192, true>
-        <<<bgrid, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
-  else if (sym)
-    i8_backward_kernel<true, Groups256, false>
-        <<<bgrid, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
-  else
-    i8_backward_kernel<false, Groups256, false>
-        <<<bgrid, kI8Threads, I8BwdSmem::kTotal, c->stream>>>(c->i8bwd_maps, ba);
+  auto bwd = sp && sym ? i8_backward_kernel<true, Groups192, true>
+             : sp        ? i8_backward_kernel<false, Groups192, true>
+             : sym       ? i8_backward_kernel<true, Groups256, false>
+                         : i8_backward_kernel<false, Groups256, false>;
+  e = launch_pdl(bwd, bgrid, dim3(kI8Threads), I8BwdSmem::kTotal, c->stream, c->i8bwd_maps, ba);
+  if (e != cudaSuccess) return e;
   prof_mark(c);
 
-  launch_tc_finalize(c, x1, d_g, 2LL * pair_tiles);
+  if ((e = launch_tc_finalize(c, x1, d_g, 2LL * pair_tiles)) != cudaSuccess) return e;
   prof_mark(c);
   count_launch(c, 7);
   return cudaGetLastError();
