@@ -151,6 +151,7 @@ SIGNATURES = {
                                        ctypes.POINTER(ctypes.c_int)]),
     "ccm_launch_count": (ctypes.c_longlong, [_vp]),
     "ccm_debug_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_longlong]),
+    "ccm_debug_set_cg_skip_padding": (ctypes.c_int, [_vp, ctypes.c_int]),
     "ccm_host_copy_bytes": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong),
                                            ctypes.POINTER(ctypes.c_longlong)]),
     "ccm_set_default_path": (None, [ctypes.c_int]),

@@ -915,6 +915,12 @@ int ccm_debug_set_wait_limit(ccm_context *c, long long cycles) {
   return CCM_OK;
 }
 
+int ccm_debug_set_cg_skip_padding(ccm_context *c, int allow) {
+  if (!c) return set_error(CCM_ERR_INVALID, "ccm_debug_set_cg_skip_padding: null context");
+  c->cg_skip_padding = allow != 0;
+  return CCM_OK;
+}
+
 const ccm_result *ccm_result_device(const ccm_context *c) { return c ? c->d_out : nullptr; }
 
 int ccm_get_result(ccm_context *c, ccm_result *out) {

@@ -35,6 +35,7 @@
 
 #include "ccm_cg_rules.cuh"
 #include "ccm_internal.cuh"
+#include "ccm_layout.cuh"
 
 namespace ccm {
 
@@ -65,20 +66,44 @@ __global__ void cg_step_kernel(const float *__restrict__ x, const float *__restr
     xt[i] = fmaf(a, s[i], x[i]);
 }
 
+// The elements a vector pass of the CG visits.  cols == 0: all n.  Else the
+// single-field block [0, nsp) and, of each of the `rows` coupling rows (stride
+// `row`), its first `cols` elements: the 21 states, the padding states skipped
+// (a solve whose x0 has zero padding states keeps them zero in x, g and s).
+// Fixed grid, fixed assignment of elements to threads.
+struct VecSpan {
+  long long n, nsp, row;
+  int rows, cols;
+};
+
+template <class F>
+__device__ __forceinline__ void for_span(const VecSpan &v, F f) {
+  const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (v.cols == 0) {
+    for (long long i = t0; i < v.n; i += stride) f(i);
+    return;
+  }
+  for (long long i = t0; i < v.nsp; i += stride) f(i);
+  for (int r = blockIdx.x; r < v.rows; r += gridDim.x) {
+    const long long base = v.nsp + (long long)r * v.row;
+    for (int c = threadIdx.x; c < v.cols; c += blockDim.x) f(base + c);
+  }
+}
+
 // Per-block FP64 partials of  a.b, a.a, a.c  (b and c may be null).  Fixed grid
 // and fixed summation order: the result does not depend on scheduling.
 __global__ void __launch_bounds__(256) cg_dots_kernel(const float *__restrict__ a,
                                                       const float *__restrict__ b,
-                                                      const float *__restrict__ c,
-                                                      long long n, double *__restrict__ part) {
+                                                      const float *__restrict__ c, VecSpan v,
+                                                      double *__restrict__ part) {
   double ab = 0.0, aa = 0.0, ac = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
+  for_span(v, [&](long long i) {
     const double av = a[i];
     if (b) ab += av * (double)b[i];
     aa += av * av;
     if (c) ac += av * (double)c[i];
-  }
+  });
   __shared__ double red[3][8];
   for (int o = 16; o > 0; o >>= 1) {
     ab += __shfl_xor_sync(0xffffffffu, ab, o);
@@ -100,13 +125,11 @@ __global__ void __launch_bounds__(256) cg_dots_kernel(const float *__restrict__ 
 
 // s <- -g (dir_mode 1) or fmaf(beta, s, -g) (dir_mode 2); dir_mode 0 keeps s.
 __global__ void cg_dir_kernel(const float *__restrict__ g, float *__restrict__ s,
-                              const CgCtl *__restrict__ ctl, long long n) {
+                              const CgCtl *__restrict__ ctl, VecSpan v) {
   const int mode = ctl->dir_mode;
   if (mode == 0) return;
   const float b = (float)ctl->beta;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    s[i] = mode == 1 ? -g[i] : fmaf(b, s[i], -g[i]);
+  for_span(v, [&](long long i) { s[i] = mode == 1 ? -g[i] : fmaf(b, s[i], -g[i]); });
 }
 
 // Sum of the partials part[i * 3 + k], i < nblocks, in a fixed order, for a block
@@ -266,11 +289,65 @@ struct CgRun {
   cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};  // whole solve | parity 0 | parity 1
   bool want_xx = false;
   bool fused = false;
+  bool padfree = false;  // x0's padding states are zero: every pass skips them
+  VecSpan span{};        // the elements the vector passes visit
   size_t mem_mark = 0;  // the context's mem_used before this solve's buffers
   int trial_kernels = 0;  // kernels of one trial (launch accounting)
 };
 
+// OR of the bit patterns of the padding states a in [21, 32) of every coupling
+// row of x into *flag.
+__global__ void cg_pad_bits_kernel(const float *__restrict__ x, long long nsp, int L,
+                                   int *__restrict__ flag) {
+  const int rows = kQ * L, pad = (kQPad - kQ) * L;
+  unsigned acc = 0;
+  for (int r = blockIdx.x; r < rows; r += gridDim.x) {
+    const unsigned *p =
+        reinterpret_cast<const unsigned *>(x + nsp + (long long)r * kQPad * L + kQ * L);
+    for (int i = threadIdx.x; i < pad; i += blockDim.x) acc |= p[i];
+  }
+  if (__any_sync(0xffffffffu, acc != 0) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
+}
+
+// The elements the solve's vector passes visit.  On the integer paths, when x0's
+// padding states are zero (checked here, or known: the batch solver starts its
+// couplings at zero), they stay zero in x, g and s (g = 2 lambda2 x there,
+// s = -g + beta s), so every pass skips them: the evaluation's column-maximum and
+// prep passes and the CG's direction and dot passes.  The work buffers' padding
+// states are zeroed once; nothing writes them afterwards.
+int choose_span(CgRun &r, bool known_zero) {
+  ccm_context *c = r.c;
+  const int L = c->L;
+  r.span = VecSpan{r.n, 0, 0, 0, 0};
+  r.padfree = false;
+  const bool i8 = c->path == CCM_PATH_TC_I8X3 || c->path == CCM_PATH_TC_I8SP;
+  if (!i8 || !c->cg_skip_padding) return CCM_OK;
+  cudaStream_t s = c->stream;
+  cudaError_t e = cudaSuccess;
+  if (!known_zero) {
+    int *d_flag = reinterpret_cast<int *>(r.d_part);
+    e = cudaMemsetAsync(d_flag, 0, sizeof(int), s);
+    if (e == cudaSuccess) {
+      cg_pad_bits_kernel<<<kDotBlocks, 256, 0, s>>>(r.xb[0], c->nsp, L, d_flag);
+      e = cudaMemcpyAsync(r.h_ctl, d_flag, sizeof(int), cudaMemcpyDeviceToHost, s);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+      return set_last_error(CCM_ERR_CUDA, "cg padding check: %s", cudaGetErrorString(e));
+    if (*reinterpret_cast<const int *>(r.h_ctl) != 0) return CCM_OK;
+  }
+  const size_t bytes = sizeof(float) * (size_t)r.n;
+  for (float *b : {r.xb[1], r.gb[0], r.gb[1], r.s})
+    if (e == cudaSuccess) e = cudaMemsetAsync(b, 0, bytes, s);
+  if (e != cudaSuccess) return set_last_error(CCM_ERR_CUDA, "cg buffers: %s", cudaGetErrorString(e));
+  r.padfree = true;
+  r.span = VecSpan{r.n, c->nsp, (long long)kQPad * L, kQ * L, kQ * L};
+  c->skip_padding = true;
+  return CCM_OK;
+}
+
 void free_run(CgRun &r) {
+  r.c->skip_padding = false;
   for (auto &g : r.exec)
     if (g) cudaGraphExecDestroy(g);
   cudaStream_t s = r.c->stream;
@@ -290,7 +367,7 @@ int enqueue_trial(CgRun &r, int p, const CgRuleParams &rp, CgHandles h) {
   cudaStream_t s = c->stream;
   float *x = r.xb[p], *xt = r.xb[1 - p], *g = r.gb[p], *gt = r.gb[1 - p];
   const long long before = c->launches;
-  cg_dir_kernel<<<grid_for(r.n), 256, 0, s>>>(g, r.s, r.d_ctl, r.n);
+  cg_dir_kernel<<<grid_for(r.n), 256, 0, s>>>(g, r.s, r.d_ctl, r.span);
   int rc;
   if (r.fused) {
     rc = enqueue_evaluation_step(c, x, r.s, &r.d_ctl->alpha, xt, gt);
@@ -299,8 +376,8 @@ int enqueue_trial(CgRun &r, int p, const CgRuleParams &rp, CgHandles h) {
     rc = enqueue_evaluation(c, xt, gt);
   }
   if (rc != CCM_OK) return rc;
-  cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(gt, r.s, g, r.n, r.d_part);
-  if (r.want_xx) cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(xt, nullptr, nullptr, r.n,
+  cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(gt, r.s, g, r.span, r.d_part);
+  if (r.want_xx) cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(xt, nullptr, nullptr, r.span,
                                                            r.d_part + 3 * kDotBlocks);
   cg_control_kernel<<<1, 256, 0, s>>>(r.d_ctl, rp, r.d_part, kDotBlocks, r.want_xx ? 1 : 0,
                                       c->d_out, nullptr, h);
@@ -560,6 +637,12 @@ int ccm::cg_graph_solve_add(ccm_context *c, float *d_x, const ccm_cg_params *par
     return set_last_error(e == cudaErrorMemoryAllocation ? CCM_ERR_NOMEM : CCM_ERR_CUDA,
                           "ccm_solve_batch: %s", cudaGetErrorString(e));
   }
+  // the batch solver starts every alignment's couplings at zero
+  if ((rc = choose_span(r, true)) != CCM_OK) {
+    free_run(r);
+    delete gs;
+    return rc;
+  }
   const bool prof = c->prof_on;
   c->prof_on = false;
   cudaStream_t s = c->stream;
@@ -571,7 +654,7 @@ int ccm::cg_graph_solve_add(ccm_context *c, float *d_x, const ccm_cg_params *par
     e = cudaStreamBeginCaptureToGraph(s, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     rc = enqueue_evaluation(c, r.xb[0], r.gb[0]);
-    cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(r.gb[0], nullptr, nullptr, r.n, r.d_part);
+    cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(r.gb[0], nullptr, nullptr, r.span, r.d_part);
     cg_start_kernel<<<1, 256, 0, s>>>(r.d_ctl, r.d_part, kDotBlocks, c->d_out, nullptr, h_out, 1);
     cudaStreamCaptureStatus cs;
     const cudaGraphNode_t *deps = nullptr;
@@ -687,6 +770,10 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
     return set_last_error(e == cudaErrorMemoryAllocation ? CCM_ERR_NOMEM : CCM_ERR_CUDA,
                           "ccm_conjugrad_gpu: %s", cudaGetErrorString(e));
   }
+  if ((rc = choose_span(r, false)) != CCM_OK) {
+    free_run(r);
+    return rc;
+  }
   // profiling marks are not captured into the solve's graphs
   const bool prof = c->prof_on;
   c->prof_on = false;
@@ -694,7 +781,7 @@ int ccm_conjugrad_gpu(ccm_context *c, float *d_x, long long n, const ccm_cg_para
   // initial evaluation at x0: f0, g0, g0.g0
   rc = enqueue_evaluation(c, r.xb[0], r.gb[0]);
   if (rc == CCM_OK) {
-    cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(r.gb[0], nullptr, nullptr, n, r.d_part);
+    cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(r.gb[0], nullptr, nullptr, r.span, r.d_part);
     cg_start_kernel<<<1, 256, 0, s>>>(r.d_ctl, r.d_part, kDotBlocks, c->d_out, nullptr, 0, 0);
     count_launch(c, 2);
     e = cudaMemcpyAsync(r.h_ctl, r.d_ctl, kCgCtlHead, cudaMemcpyDeviceToHost, s);
@@ -764,6 +851,7 @@ int ccm::conjugrad_callback_gpu(float *d_x, long long n, ccm_eval_callback eval,
   const CgRuleParams rp = rule_params(*params);
   cudaStream_t s = 0;  // legacy default stream
   const size_t bytes = sizeof(float) * (size_t)n;
+  const VecSpan flat{n, 0, 0, 0, 0};  // a foreign evaluation: every element
   float *xb[2] = {d_x, nullptr}, *gb[2] = {nullptr, nullptr}, *dir = nullptr;
   CgCtl *d_ctl = nullptr;
   double *d_part = nullptr, *d_f = nullptr;
@@ -788,19 +876,19 @@ int ccm::conjugrad_callback_gpu(float *d_x, long long n, ccm_eval_callback eval,
   };
   if (e == cudaSuccess) e = evaluate(0);
   if (e == cudaSuccess) {
-    cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(gb[0], nullptr, nullptr, n, d_part);
+    cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(gb[0], nullptr, nullptr, flat, d_part);
     cg_start_kernel<<<1, 256, 0, s>>>(d_ctl, d_part, kDotBlocks, nullptr, d_f, 0, 0);
     e = cudaMemcpyAsync(h, d_ctl, kCgCtlHead, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   }
   while (e == cudaSuccess && h->status == kCgRunning) {
     const int p = h->parity, iter0 = h->iter;
-    cg_dir_kernel<<<grid_for(n), 256, 0, s>>>(gb[p], dir, d_ctl, n);
+    cg_dir_kernel<<<grid_for(n), 256, 0, s>>>(gb[p], dir, d_ctl, flat);
     cg_step_kernel<<<grid_for(n), 256, 0, s>>>(xb[p], dir, &d_ctl->alpha, xb[1 - p], n);
     e = evaluate(1 - p);
     if (e != cudaSuccess) break;
-    cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(gb[1 - p], dir, gb[p], n, d_part);
-    if (progress) cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(xb[1 - p], nullptr, nullptr, n,
+    cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(gb[1 - p], dir, gb[p], flat, d_part);
+    if (progress) cg_dots_kernel<<<kDotBlocks, 256, 0, s>>>(xb[1 - p], nullptr, nullptr, flat,
                                                            d_part + 3 * kDotBlocks);
     cg_control_kernel<<<1, 256, 0, s>>>(d_ctl, rp, d_part, kDotBlocks, progress ? 1 : 0, nullptr,
                                         d_f, none);

@@ -75,6 +75,7 @@ struct I8PrepArgs {
   float inv_L;
   float lambda_pair;
   float g2_coef;
+  int ncols;  // elements of a row that prep reads and writes: 32 L, or 21 L (padding skipped)
 };
 
 struct I8FwdArgs {
@@ -285,6 +286,11 @@ struct ccm_context {
   int8_t *d_wdig[3] = {nullptr, nullptr, nullptr};     // S x S digits of W
   int8_t *d_rdig[3] = {nullptr, nullptr, nullptr};     // Npad x S digits of R
   uint32_t *d_colmax = nullptr;  // 21 L column maxima of |W|, then S per-slot encoding factors
+  // the column-maximum and prep passes skip the padding states a >= 21 (set by a
+  // device-side solve whose x0 has zero padding states, while it captures and
+  // runs; ccm_debug_set_cg_skip_padding clears cg_skip_padding to forbid it)
+  bool skip_padding = false;
+  bool cg_skip_padding = true;
   ccm::I8FwdMaps i8fwd_maps;
   ccm::I8BwdMaps i8bwd_maps;
   // sparse integer forward: W digits are KP x SW (K rows l * 21 + q, 192-slot

@@ -63,6 +63,8 @@ __device__ __forceinline__ int col_exponent(uint32_t mbits) {
 // (bx, by): 256 consecutive columns c of a 32 L row, rows [by*R, by*R + R).
 // STEP = true also takes the CG trial step: v = fmaf(alpha, s, x) is written to
 // xt for every element of x (the last row of blocks steps the single fields).
+// cols = 21 L instead of 32 L leaves out the padding states (a solve that keeps
+// them zero in x, s and xt).
 template <bool STEP>
 __global__ void __launch_bounds__(256) i8_colmax_kernel(const float *__restrict__ x,
                                                         const float *__restrict__ s,
@@ -70,7 +72,7 @@ __global__ void __launch_bounds__(256) i8_colmax_kernel(const float *__restrict_
                                                         float *__restrict__ xt,
                                                         uint32_t *__restrict__ colmax, int L,
                                                         long long nsp, int rows_per_block,
-                                                        int krow_order) {
+                                                        int krow_order, int cols) {
   griddep_wait();
   griddep_launch();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -79,11 +81,12 @@ __global__ void __launch_bounds__(256) i8_colmax_kernel(const float *__restrict_
   if (STEP) {
     a = (float)alpha[0];
     if (blockIdx.y == gridDim.y - 1) {
-      if (c < nsp) xt[c] = fmaf(a, s[c], x[c]);
+      for (long long i = c; i < nsp; i += (long long)gridDim.x * blockDim.x)
+        xt[i] = fmaf(a, s[i], x[i]);
       return;
     }
   }
-  if (c >= w32) return;
+  if (c >= cols) return;  // cols = 32 L, or 21 L when the padding states are skipped
   const int r0 = blockIdx.y * rows_per_block;
   const int r1 = min(r0 + rows_per_block, kQ * L);
   float m = 0.0f;
@@ -180,7 +183,7 @@ __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ 
   if ((L & 3) == 0) {
     const float4 *src = reinterpret_cast<const float4 *>(x2 + base);
     float4 *dst = reinterpret_cast<float4 *>(g2 + base);
-    const int n4 = kQPad * L / 4, nreal4 = nreal / 4;
+    const int n4 = args.ncols / 4, nreal4 = nreal / 4;
     constexpr int kU = 4;
     for (int i0 = threadIdx.x; i0 < n4; i0 += kU * blockDim.x) {
       float4 v[kU];
@@ -212,7 +215,7 @@ __global__ void __launch_bounds__(256) i8_prep_kernel(const float *__restrict__ 
       }
     }
   } else {
-    for (int i = threadIdx.x; i < kQPad * L; i += blockDim.x) {
+    for (int i = threadIdx.x; i < args.ncols; i += blockDim.x) {
       const float v = x2[base + i];
       acc += (double)v * v;
       if (i < nreal) xrow[G::slot_of(i / L, i % L)] = v;
@@ -1344,14 +1347,15 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   prof_mark(c);
   if ((e = zero_words(c->d_colmax, (long long)kQ * L, c->stream)) != cudaSuccess) return e;
   constexpr int kRows = 32;
-  const dim3 cgrid((kQPad * L + 255) / 256, (kQ * L + kRows - 1) / kRows + (step ? 1 : 0));
+  const int cols = (c->skip_padding ? kQ : kQPad) * L;
+  const dim3 cgrid((cols + 255) / 256, (kQ * L + kRows - 1) / kRows + (step ? 1 : 0));
   if (step)
     e = launch_pdl(i8_colmax_kernel<true>, cgrid, dim3(256), 0, c->stream, d_x, d_s, d_alpha, d_xt,
-                   c->d_colmax, L, c->nsp, kRows, sp ? 1 : 0);
+                   c->d_colmax, L, c->nsp, kRows, sp ? 1 : 0, cols);
   else
     e = launch_pdl(i8_colmax_kernel<false>, cgrid, dim3(256), 0, c->stream, d_x,
                    (const float *)nullptr, (const double *)nullptr, (float *)nullptr, c->d_colmax,
-                   L, c->nsp, kRows, sp ? 1 : 0);
+                   L, c->nsp, kRows, sp ? 1 : 0, cols);
   if (e != cudaSuccess) return e;
   // per-slot factors after the column maxima, 16-byte aligned for the float4 loads
   float *enc = reinterpret_cast<float *>(c->d_colmax + ((kQ * L + 3) & ~3));
@@ -1372,6 +1376,7 @@ cudaError_t i8_evaluate(ccm_context *c, const float *d_x, float *d_g, const floa
   pa.L = L; pa.S = wcols; pa.KB = c->KP / 128; pa.lambda_pair = c->lambda_pair;
   pa.g2_coef = c->gradient == CCM_GRADIENT_PARTIAL ? 1.0f : 2.0f;
   pa.inv_L = 1.0f / (float)L;
+  pa.ncols = cols;
   if (sp)
     e = launch_pdl(i8_prep_kernel<Groups192, true>, dim3(kQ * L), dim3(256), sizeof(float) * wcols,
                    c->stream, x2, g2, pa);

@@ -210,6 +210,13 @@ CCM_API long long ccm_debug_copy(ccm_context *ctx, int which, void *dst, long lo
  * reference (which has no bounded waits). */
 CCM_API int ccm_debug_set_wait_limit(ccm_context *ctx, long long cycles);
 
+/* Integer paths: a device-side solve (ccm_conjugrad_gpu, ccm_solve_batch) whose
+ * x0 has zero padding states (a in [21, 32) of every coupling row; always so on
+ * the reference's CLI path) keeps them zero and skips them in every vector pass
+ * (allow = 1, the default).  allow = 0 makes the solve visit every element, for
+ * comparisons; results agree up to the summation order of the FP64 dots. */
+CCM_API int ccm_debug_set_cg_skip_padding(ccm_context *ctx, int allow);
+
 /* Allocation-free sequence reweighting.  No counterpart in the reference.
  *
  * For callers that must not allocate device memory: a process whose memory

@@ -124,3 +124,41 @@ def test_whole_solve_graph_equals_per_iteration_loop(gpu, oracle_mod, path):
                                                           max_iter=40, eps=1e-3)
     assert ra.status == st_h and ra.iterations == it_h and ra.evaluations == ev_h
     assert abs(ra.fx - fh[-1]) / abs(fh[-1]) < 2e-5
+
+
+@pytest.mark.parametrize("path", ["tc_i8sp", "tc_i8x3"])
+@pytest.mark.parametrize("whole_solve", [True, False])
+def test_padding_free_passes(gpu, path, whole_solve):
+    """x0 with zero padding states: the solve keeps them exactly zero and its vector
+    passes skip them; the trajectory equals that of a solve visiting every element
+    (up to the summation order of the FP64 dots).  x0 with a nonzero padding state:
+    the check sees it and the solve visits every element, bit for bit as when
+    skipping is forbidden.  whole_solve=False: the per-iteration graphs (a progress
+    callback)."""
+    import torch
+    from ccmpred_b200 import lib, nsingle_padded
+    msa = synth.generate(synth.MSAConfig("pad", 37, 500, n_pairs=3, seed=67))
+    L = msa.shape[1]
+    nsp = nsingle_padded(L)
+    progress = None if whole_solve else (lambda *a: False)
+
+    def solve(x0, allow):
+        with Evaluator(msa, path=path) as ev:
+            assert lib().ccm_debug_set_cg_skip_padding(ev.handle, allow) == 0
+            xd = torch.from_numpy(x0.copy()).cuda()
+            res = ev.minimize(xd, max_iterations=10, epsilon=0.0, progress=progress)
+            return res, xd.cpu().numpy()
+
+    x0 = init_bias(msa)
+    r1, x1 = solve(x0, 1)
+    r0, xz = solve(x0, 0)
+    assert r1.iterations == r0.iterations == 10 and r1.evaluations == r0.evaluations
+    assert abs(r1.fx - r0.fx) <= 1e-9 * abs(r0.fx)
+    np.testing.assert_allclose(x1, xz, rtol=0, atol=1e-6)
+    pad = x1[nsp:].reshape(21, L, 32, L)[:, :, 21:, :]
+    assert not np.any(pad.view(np.uint32))                 # still exactly +0.0
+    xp = x0.copy()
+    xp[nsp:].reshape(21, L, 32, L)[3, 5, 25, 7] = 1e-3      # one nonzero padding state
+    rp1, xp1 = solve(xp, 1)
+    rp0, xp0 = solve(xp, 0)
+    assert rp1.fx == rp0.fx and np.array_equal(xp1.view(np.uint32), xp0.view(np.uint32))
