@@ -443,6 +443,8 @@ def run_large(args, world, rank, local):
     _lib.check(lib.ccm_profile_end(ev.handle, kms, 8, ctypes.byref(nk), ctypes.byref(ne)))
     names = ["prep", "forward", "backward", "finalize"]
     kernels = {names[i]: kms[i] / max(ne.value, 1) for i in range(min(nk.value, 4))}
+    f_x0 = ev.evaluate(x0, g)
+    gnorm_x0 = float(torch.linalg.vector_norm(g.double()))
     torch.cuda.synchronize()
     xs = x0.clone()
     launches0 = lib.ccm_launch_count(ev.handle)
@@ -519,6 +521,9 @@ def run_large(args, world, rank, local):
                      "flops_per_evaluation": flops_eval,
                      "note": "useful FLOPs of both contractions per evaluation over the whole "
                              "solve's time (CG vector passes and graph overhead included)"},
+        "objective": {"f_x0": f_x0, "gnorm_x0": gnorm_x0, "f_final": f64,
+                      "gnorm_final": float(nrm(g64)),
+                      "note": "f and ||g|| at x0 (this path) and at the final x (FP64 path)"},
         "precision_at_final_x": {
             args.path: prec(f_tc, g_tc), "simt_f32": prec(f32, g32),
             "reference": "FP64 CUDA-core path (simt_f64) at the same x"},

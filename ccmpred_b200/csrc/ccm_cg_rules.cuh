@@ -14,7 +14,11 @@
 //     curvature (C):            g_t.s >= wolfe g.s        (g.s < 0)
 //     A and C                  -> accept
 //     A, not C (slope still steep: the step is short), two trials left
-//                              -> remember alpha, try alpha / alpha_mul
+//                              -> remember alpha, try the secant step
+//                                 alpha g.s / (g.s - g_t.s), the zero of the
+//                                 line through the two slopes, kept in
+//                                 [1.5, 16] alpha (alpha / alpha_mul when
+//                                 g_t.s <= g.s, no zero ahead)
 //     A, not C, fewer trials   -> accept
 //     not A after an expansion -> retreat: the remembered step once more
 //                                 (it met A; the trial repeats it exactly, and
@@ -83,6 +87,16 @@ static_assert(offsetof(CgCtl, fhist) == kCgCtlHead, "CgCtl: scalars before fhist
 
 __host__ __device__ inline bool cg_finite(double v) { return v - v == 0.0; }
 
+// Growth of a step that met sufficient decrease with the slope gts at x_t still
+// steeper than wolfe gs (gs < 0): the secant estimate of where the slope along s
+// reaches zero, gs / (gs - gts) of the step, limited to [kCgGrowMin, kCgGrowMax];
+// 1 / alpha_mul when gts <= gs (the slope has not risen: no zero ahead).
+constexpr double kCgGrowMin = 1.5, kCgGrowMax = 16.0;
+__host__ __device__ inline double cg_expansion(double gs, double gts, double alpha_mul) {
+  if (!(gts > gs)) return 1.0 / alpha_mul;
+  return fmin(fmax(gs / (gs - gts), kCgGrowMin), kCgGrowMax);
+}
+
 // After the initial evaluation at x0 (f0, g0.g0).
 __host__ __device__ inline void cg_rules_start(CgCtl &c, double f0, double gg0) {
   c.f = f0;
@@ -144,7 +158,7 @@ __host__ __device__ inline bool cg_rules_trial(CgCtl &c, const CgTrial &t, const
     accept = true;
   } else if (suff) {
     c.alpha_good = c.alpha;  // expand: the slope at x_t is still steep
-    c.alpha = c.alpha / p.alpha_mul;
+    c.alpha = c.alpha * cg_expansion(c.gs, t.gts, p.alpha_mul);
   } else if (c.alpha_good > 0.0) {
     c.alpha = c.alpha_good;  // the expansion overshot: back to the good step
     c.retreat = 1;

@@ -192,7 +192,9 @@ void oracle_calculate_weights(const unsigned char *msa, int L, int N, float thre
  *   a trial x_t = x + alpha s meets (A) f_t <= f + ftol alpha g.s and
  *   (C) g_t.s >= wolfe g.s (wolfe <= 0: C always holds);
  *   A and C, or A with fewer than two trials left: take the step;
- *   A without C and two trials left: remember alpha, try alpha / alpha_mul;
+ *   A without C and two trials left: remember alpha, try the secant step
+ *   alpha g.s / (g.s - g_t.s) kept in [1.5, 16] alpha (alpha / alpha_mul when
+ *   g_t.s <= g.s);
  *   not A after such an expansion: retreat to the remembered alpha (taken);
  *   not A otherwise: safeguarded quadratic backtracking in [0.1, alpha_mul] alpha;
  *   max_ls trials without a step: restart along -g once (fresh budget), then fail;
@@ -233,14 +235,20 @@ int oracle_conjugrad_f64(const unsigned char *msa, const double *w, int L, int N
 			evals++;
 			ls++;
 			const int suff = isfinite(ft) && ft <= f + ftol * alpha * gs;
-			const int curv = wolfe <= 0.0 || dot(gt, s, n) >= wolfe * gs;
+			const double gts = dot(gt, s, n);
+			const int curv = wolfe <= 0.0 || gts >= wolfe * gs;
 			if (retreat) {
 				ok = suff;
 			} else if (suff && (curv || ls + 2 > max_ls)) {
 				ok = 1;
 			} else if (suff) {
 				good = alpha;
-				alpha = alpha / alpha_mul;
+				if (gts > gs) {
+					const double r = gs / (gs - gts);
+					alpha = alpha * (r < 1.5 ? 1.5 : (r > 16.0 ? 16.0 : r));
+				} else {
+					alpha = alpha / alpha_mul;
+				}
 			} else if (good > 0.0) {
 				alpha = good;
 				retreat = 1;
