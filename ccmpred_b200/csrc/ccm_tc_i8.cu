@@ -346,7 +346,21 @@ struct I8FwdSmem {
 // the merge then releases both accumulators, so that the next tile's MMAs run
 // during passes B and C.  TILED: the digits of R go to the backward's tiled
 // storage (i8_bwd_tile_offset) instead of row-major Npad x S.
-template <class G, int H, bool REGS = false, bool TILED = false>
+// hi * 2^14 + lo, rounded once to float.  A row of the one-hot operand holds L
+// ones, so |hi| <= 128 L and 0 <= lo <= 16383 L: with L <= kI8NarrowMaxL the exact
+// sum lies in [-2^31, 2^31) and the 32-bit conversion (NARROW) gives the float the
+// 64-bit one gives.
+constexpr int kI8NarrowMaxL = 1024;
+template <bool NARROW>
+__device__ __forceinline__ float i8_merge_digits(uint32_t hi, uint32_t lo) {
+  if constexpr (NARROW) {
+    return __int2float_rn((int)(hi * 16384u + lo));
+  } else {
+    return __ll2float_rn((long long)(int)hi * 16384 + (long long)(int)lo);
+  }
+}
+
+template <class G, int H, bool REGS = false, bool TILED = false, bool NARROW = false>
 __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint32_t t_hi,
                                                      uint32_t t_lo, const float *tab_scale,
                                                      const float *tab_v, float *xbuf, int q,
@@ -385,8 +399,7 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
         const int col = cc * 16 + i;
-        const long long qs = (long long)(int)vh[i] * 16384 + (long long)(int)vl[i];
-        const float z = fmaf(__ll2float_rn(qs), tab_scale[col], tab_v[col]);
+        const float z = fmaf(i8_merge_digits<NARROW>(vh[i], vl[i]), tab_scale[col], tab_v[col]);
         if (c < 2) st[c * 16 + i] = __float_as_uint(z);
         else zr[(c - 2) * 16 + i] = __float_as_uint(z);
         if (col < kGroupUsed) {
@@ -409,8 +422,7 @@ __device__ __forceinline__ void i8_fwd_epilogue_tile(const I8FwdArgs &args, uint
 #pragma unroll
     for (int i = 0; i < 32; ++i) {
       const int col = cc * 32 + i;
-      const long long qs = (long long)(int)vh[i] * 16384 + (long long)(int)vl[i];
-      const float z = fmaf(__ll2float_rn(qs), tab_scale[col], tab_v[col]);
+      const float z = fmaf(i8_merge_digits<NARROW>(vh[i], vl[i]), tab_scale[col], tab_v[col]);
       vh[i] = __float_as_uint(z);
       if (col < kGroupUsed) {
         const int a = col / kGroupCols, jj = col % kGroupCols;
@@ -746,9 +758,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
       tc_fence_after();
       const uint32_t lq = (uint32_t)(q * 32) << 16;
       const long long part = (long long)tile * 2 + rank;
-      if (half == 0)
+      const bool narrow = L <= kI8NarrowMaxL;
+      if (half == 0 && narrow)
+        i8_fwd_epilogue_tile<Groups256, 0, false, false, true>(args, t_hi + lq, t_lo + lq, tab_scale,
+                                                           tab_v, xbuf, q, lane, n, t, part, lo_bar);
+      else if (half == 0)
         i8_fwd_epilogue_tile<Groups256, 0>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v, xbuf, q, lane, n, t,
                                 part, lo_bar);
+      else if (narrow)
+        i8_fwd_epilogue_tile<Groups256, 1, false, false, true>(args, t_hi + lq, t_lo + lq, tab_scale,
+                                                           tab_v, xbuf, q, lane, n, t, part, lo_bar);
       else
         i8_fwd_epilogue_tile<Groups256, 1>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v, xbuf, q, lane, n, t,
                                 part, lo_bar);
@@ -1028,10 +1047,19 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kI8Threads, 1)
       const uint32_t lq = (uint32_t)(q * 32) << 16;
       const long long part = (long long)tile * 2 + rank;
       // both accumulators are released inside, right after the merge
-      if (half == 0)
+      const bool narrow = L <= kI8NarrowMaxL;
+      if (half == 0 && narrow)
+        i8_fwd_epilogue_tile<Groups192, 0, true, true, true>(args, t_hi + lq, t_lo + lq, tab_scale,
+                                                       tab_v, xbuf, q, lane, n, t, part, empty_bar,
+                                                       t_stash + lq);
+      else if (half == 0)
         i8_fwd_epilogue_tile<Groups192, 0, true, true>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v,
                                                  xbuf, q, lane, n, t, part, empty_bar,
                                                  t_stash + lq);
+      else if (narrow)
+        i8_fwd_epilogue_tile<Groups192, 1, true, true, true>(args, t_hi + lq, t_lo + lq, tab_scale,
+                                                       tab_v, xbuf, q, lane, n, t, part, empty_bar,
+                                                       t_stash + 32 + lq);
       else
         i8_fwd_epilogue_tile<Groups192, 1, true, true>(args, t_hi + lq, t_lo + lq, tab_scale, tab_v,
                                                  xbuf, q, lane, n, t, part, empty_bar,
