@@ -130,6 +130,37 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
+def tensor_peak(peaks, peak_kind, clocks, elapsed_ms):
+    """The bf16 denominator for a tensor-bound kernel: the burst figure (measured at
+    the maximum SM clock) or the sustained one (measured under the power cap, at the
+    lower clock recorded beside it), whichever was taken at the clock nearer the
+    median SM clock this timed region held.  Without clock samples, the length of
+    the timed region decides (a region under a second keeps the maximum clock).
+    Returns (peak, name, why)."""
+    burst = float(peaks.get("bf16_tflops", peaks.get("bf16_tflops_sustained")))
+    sustained = float(peaks.get("bf16_tflops_sustained", burst))
+    f_burst = float(peaks.get("sm_max_mhz") or 1965.0)
+    f_sus = (peaks.get("clocks_under_load") or {}).get("sm_mhz_median")
+    held = (clocks or {}).get("sm_mhz")
+    if held and f_sus:
+        mid = 0.5 * (f_burst + float(f_sus))
+        if held >= mid:
+            peak, name = burst, "bf16_tflops"
+            why = f"burst: median SM clock {held:.0f} MHz, nearer {f_burst:.0f} than {f_sus:.0f}"
+        else:
+            peak, name = sustained, "bf16_tflops_sustained"
+            why = f"sustained: median SM clock {held:.0f} MHz, nearer {f_sus:.0f} than {f_burst:.0f}"
+    elif elapsed_ms < 1000.0:
+        peak, name = burst, "bf16_tflops"
+        why = f"burst: timed region {elapsed_ms:.0f} ms < 1 s, no clock samples"
+    else:
+        peak, name = sustained, "bf16_tflops_sustained"
+        why = f"sustained: timed region {elapsed_ms:.0f} ms >= 1 s, no clock samples"
+    if peak_kind == "fallback":
+        why += "; MEASURED_PEAKS.json absent"
+    return peak, name, why
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -486,7 +517,7 @@ def run_large(args, world, rank, local):
                 "g1_rel_of_g": float(nrm(d[:20 * L]) / nrm(g64)),
                 "g2_rel_of_g": float(nrm(d[nsp:]) / nrm(g64))}
     peaks, peak_kind = measured_peaks()
-    peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
+    peak, peak_name, peak_why = tensor_peak(peaks, peak_kind, clocks, elapsed_ms)
     flops_eval = 4.0 * N * (21 * L) ** 2
     achieved = flops_eval * res.evaluations / (elapsed_ms / 1e3) / 1e12
     its = max(res.iterations, 1)
@@ -517,7 +548,7 @@ def run_large(args, world, rank, local):
         "evals_per_s": res.evaluations / (elapsed_ms / 1e3), "cg_status": res.status,
         "kernels_ms_per_evaluation": kernels,
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "peak_source": f"{peak_kind} bf16_tflops_sustained",
+                     "frac": achieved / peak, "peak_source": f"{peak_kind} {peak_name} ({peak_why})",
                      "flops_per_evaluation": flops_eval,
                      "note": "useful FLOPs of both contractions per evaluation over the whole "
                              "solve's time (CG vector passes and graph overhead included)"},
@@ -629,16 +660,7 @@ def main():
         peaks, peak_kind = measured_peaks()
         peak_burst = float(peaks.get("bf16_tflops", peaks.get("bf16_tflops_sustained")))
         peak_sustained = float(peaks.get("bf16_tflops_sustained", peak_burst))
-        # the burst figure for a timed region shorter than a second (clocks stay at
-        # their maximum), the sustained one (under the power cap) for longer runs
-        if elapsed_ms < 1000.0:
-            peak, peak_name = peak_burst, "bf16_tflops"
-            peak_why = f"burst: timed region {elapsed_ms:.0f} ms < 1 s"
-        else:
-            peak, peak_name = peak_sustained, "bf16_tflops_sustained"
-            peak_why = f"sustained: timed region {elapsed_ms:.0f} ms >= 1 s"
-        if peak_kind == "fallback":
-            peak_why += "; MEASURED_PEAKS.json absent"
+        peak, peak_name, peak_why = tensor_peak(peaks, peak_kind, clocks, elapsed_ms)
 
         flops = 2.0 * N * (21 * L) ** 2
         dom = max(("tc_forward", "tc_backward"), key=lambda k: kernels.get(k, 0.0))

@@ -31,3 +31,22 @@ def test_reference_arm_prints_one_json_line(ref_mod):
     # the same workload keys as the GPU arm's config, nothing about the implementation
     assert {"ncol", "nrow", "planted_pairs", "seed", "parallelism"} <= set(d["config"])
     assert "path" not in d["config"]
+
+
+def test_tensor_peak_follows_the_held_clock():
+    """The roofline's bf16 denominator is the measured peak taken at the clock nearer
+    the one the timed region held: burst near the maximum clock, sustained near the
+    power-capped clock; the region's length decides only without clock samples."""
+    sys.path.insert(0, ROOT)
+    import bench
+    peaks = {"bf16_tflops": 1672.5, "bf16_tflops_sustained": 1395.1, "sm_max_mhz": 1965.0,
+             "clocks_under_load": {"sm_mhz_median": 1342.0}}
+    peak, name, why = bench.tensor_peak(peaks, "measured", {"sm_mhz": 1882.0}, 1004.0)
+    assert (peak, name) == (1672.5, "bf16_tflops") and "1882" in why
+    peak, name, _ = bench.tensor_peak(peaks, "measured", {"sm_mhz": 1500.0}, 10.0)
+    assert (peak, name) == (1395.1, "bf16_tflops_sustained")
+    assert bench.tensor_peak(peaks, "measured", None, 20.0)[1] == "bf16_tflops"
+    assert bench.tensor_peak(peaks, "measured", None, 2000.0)[1] == "bf16_tflops_sustained"
+    fb = bench.tensor_peak({"bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0},
+                           "fallback", {"sm_mhz": 1965.0}, 5.0)
+    assert fb[0] == 1590.0 and "absent" in fb[2]
