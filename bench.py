@@ -5,9 +5,11 @@ One step = one evaluation of f and the full gradient at a fixed parameter
 vector x (the reference's evaluate callback, src/evaluate_cuda.c:23-74),
 through the C ABI of libccmpred_b200.so.
 
-  value       evals/s of the split-bf16 tensor-core path with x and g resident
-              in HBM (ccm_evaluate_async back to back, CUDA events on the
-              context stream, max over ranks);
+  value       evals/s of the default path (--path, tc_i8sp: 8-bit fixed-point
+              digits with exact integer sums on the tensor cores) with x and g
+              resident in HBM (ccm_evaluate_async back to back, CUDA events on
+              the context stream, max over ranks); the split-bf16 path the
+              metric names is timed beside it (tc_bf16x2);
   e2e         evals/s through the host-pointer C ABI (ccm_evaluate_host):
               every step copies x host->device from pinned memory and g + f
               device->host;
@@ -17,7 +19,9 @@ through the C ABI of libccmpred_b200.so.
   plain_f32   the same metric on the plain FP32 CUDA-core path (no tensor cores);
   precision   errors of f and g against the FP64 oracle at the same x;
   cpu_baseline the reference's evaluate_cpu_omp (compiled from its sources)
-              on a bounded sample, on this host's cores.
+              on a bounded sample, on this host's cores;
+  batch256, L1000_N20000  (N=1, after the timed region; --no-extras skips them)
+              the lines of --workload batch256 and --workload L1000_N20000.
 
 `--impl reference` times the reference's own CPU implementation
 (evaluate_cpu_omp, all host threads) on the same workload instead.
